@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Benchmark of the distributed-scatterer chain (KS -> coherence -> EMI -> temporal coherence).
+
+Metric: DS pixels per second through the whole chain on one synthetic stack (the
+2000 x 2000 x 100 complex64 scene with an 11 x 21 window by default), i.e. the number of
+DS points whose phase history and temporal coherence are produced, divided by the time
+of one pass over the stack (intensity, KS test + SHP selection over every pixel, DS
+extraction, coherence, EMI, temporal coherence).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank processes its own stack (tiles are
+independent: no collective on the data path) and ``value`` is the sum over ranks,
+timed as the max over ranks. ``--impl reference`` times the host restatement of the
+reference algorithm (the oracle port) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "DS pixels/s (KS->coh->EMI->tcoh)"
+UNIT = "DS pixels/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--size", type=int, default=0, help="override nlines = width (smaller runs)")
+    ap.add_argument("--precision", default="fp32")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=160, help="side of the crop timed on the host")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- peaks
+def measured_peaks() -> dict:
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        d["source"] = "measured"
+        return d
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+# ----------------------------------------------------------------------------- CPU leg
+def cpu_chain_rate(cfg, rslc_np, side: int, nthreads: int):
+    """Oracle chain on a side x side crop of the stack; DS pixels per second on the host."""
+    from oracle import oracle as O  # noqa: PLC0415
+    from concurrent.futures import ThreadPoolExecutor  # noqa: PLC0415
+
+    crop = np.ascontiguousarray(rslc_np[:side, :side])
+    t0 = time.perf_counter()
+    rmli = O.intensity(crop)
+    p = O.ks_test(rmli, cfg.az_half_win, cfg.r_half_win, nthreads=nthreads)
+    is_shp, num = O.select_shp(p, cfg.p_max)
+    idx, pc = O.ds_candidates(is_shp, num, cfg.min_shp)
+    coh = O.emperical_co_pc(crop, idx, pc, nthreads=nthreads).astype(np.complex64)
+    chunks = [coh[i:i + 256] for i in range(0, len(coh), 256)]
+    with ThreadPoolExecutor(nthreads) as ex:
+        res = list(ex.map(lambda c: O.emi(c), chunks))
+    ph = np.concatenate([r[0] for r in res]) if res else np.zeros((0, crop.shape[2]), np.complex128)
+    O.ds_temp_coh(coh, ph.astype(np.complex64), nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return len(idx) / dt, dt, len(idx)
+
+
+# ----------------------------------------------------------------------------- main
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    from moraine_b200.synth import CONFIGS  # noqa: PLC0415
+
+    cfg = CONFIGS[args.config]
+    if args.size:
+        cfg = cfg.scaled(nlines=args.size, width=args.size,
+                         n_patches=max(8, cfg.n_patches * args.size * args.size // (cfg.nlines * cfg.width)))
+    workload = {"workload": f"ds-chain {cfg.name} {cfg.nlines}x{cfg.width}x{cfg.nimages} complex64, "
+                            f"window {cfg.az_win}x{cfg.r_win}, p<{cfg.p_max}, DS = SHP count >= {cfg.min_shp}",
+                "nlines": cfg.nlines, "width": cfg.width, "nimages": cfg.nimages,
+                "window": [cfg.az_win, cfg.r_win], "precision": args.precision,
+                "l2": "inputs larger than L2 (stack, masks and coherence batch each exceed 126 MB)"
+                      if cfg.nlines * cfg.width * cfg.nimages * 8 > 126e6 else "small input (fits L2)",
+                "parallelism": f"independent tiles x{args.gpus}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        import torch  # noqa: PLC0415
+        from moraine_b200.synth import make_stack  # noqa: PLC0415
+
+        nthreads = len(os.sched_getaffinity(0))
+        side = min(args.cpu_sample, cfg.nlines)
+        sub = cfg.scaled(nlines=side, width=side,
+                         n_patches=max(4, cfg.n_patches * side * side // (cfg.nlines * cfg.width)))
+        z = make_stack(sub).numpy()
+        for _ in range(max(1, args.warmup if args.warmup < 2 else 1)):
+            cpu_chain_rate(cfg, z[:48, :48], 48, nthreads)  # warm caches / thread pools
+        rates, times, nds = [], [], []
+        for _ in range(args.steps):
+            r, dt, n = cpu_chain_rate(cfg, z, side, nthreads)
+            rates.append(r)
+            times.append(dt)
+            nds.append(n)
+        value = float(np.sum(nds) / np.sum(times))
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/c64 (f64 accumulate)",
+            "data": "synthetic", "config": workload,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
+                             "sample": f"{side}x{side} crop of the scene model per step ({int(np.mean(nds))} DS "
+                                       f"points), oracle chain: C/OpenMP KS, Gram and temp_coh, numpy LAPACK EMI"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+
+    import torch  # noqa: PLC0415
+    import torch.distributed as dist  # noqa: PLC0415
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta  # noqa: PLC0415
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    from moraine_b200 import _lib  # noqa: PLC0415
+    from moraine_b200.chain import DsChain  # noqa: PLC0415
+    from moraine_b200.synth import make_stack  # noqa: PLC0415
+
+    _lib.load()
+    rcfg = cfg.scaled(seed=cfg.seed + 1000 * rank)
+    rslc = make_stack(rcfg, device=dev)
+    torch.cuda.synchronize()
+    chain = DsChain(cfg.nlines, cfg.width, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp,
+                    precision=args.precision, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        res = chain.run(rslc)
+    n_ds = res.n_ds
+
+    # per-stage split (separate pass with events, outside the timed region)
+    chain.timing = True
+    stage = chain.run(rslc).stage_ms
+    chain.timing = False
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(args.steps):
+        res = chain.run(rslc)
+    t1.record()
+    barrier()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms, float(n_ds)], device=dev, dtype=torch.float64)
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        ms_max, ds_total = float(tmax[0]), float(t[1])
+    else:
+        ms_max, ds_total = ms, float(n_ds)
+    value = ds_total / (ms_max / 1e3)
+
+    # end to end through the public chain API from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(rslc.shape, dtype=rslc.dtype, pin_memory=True)
+        host.copy_(rslc)
+        out_ph = torch.empty((chain.shape[0] * chain.shape[1], cfg.nimages), dtype=torch.complex64, pin_memory=True)
+        out_q = torch.empty((chain.shape[0] * chain.shape[1],), dtype=torch.float32, pin_memory=True)
+        out_t = torch.empty_like(out_q)
+        out_idx = torch.empty((chain.shape[0] * chain.shape[1], 2), dtype=torch.int32, pin_memory=True)
+        dev_in = torch.empty_like(rslc)
+        d2h = 0
+
+        def e2e_step():
+            dev_in.copy_(host, non_blocking=True)
+            r = chain.run(dev_in)
+            n = r.n_ds
+            out_ph[:n].copy_(r.ph, non_blocking=True)
+            out_q[:n].copy_(r.quality, non_blocking=True)
+            out_t[:n].copy_(r.t_coh, non_blocking=True)
+            out_idx[:n].copy_(r.idx, non_blocking=True)
+            return n * (cfg.nimages * 8 + 4 + 4 + 8)
+
+        e2e_step()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            d2h = e2e_step()
+        e1.record()
+        barrier()
+        ems = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            t = torch.tensor([ems], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t[0])
+        e2e = {"value": ds_total / (ems / 1e3), "unit": UNIT, "ms_per_step": ems,
+               "h2d_bytes_per_step": int(rslc.numel() * 8), "d2h_bytes_per_step": int(d2h + 8),
+               "path": "moraine_b200.chain.DsChain.run on a pinned host stack, results copied back"}
+
+    # roofline of the dominant stage (filled by kernel-level timing in the stage split)
+    peaks = measured_peaks()
+    dom = max(stage, key=stage.get) if stage else None
+    roofline = None
+    if dom:
+        N = cfg.nimages
+        dom_ms = stage[dom]
+        if dom == "emi_tcoh":
+            flops = n_ds * (2.7 * N ** 3 + 80 * N ** 2)
+            achieved = flops / (dom_ms / 1e3) / 1e12
+            roofline = {"kernel": "emi_kernel", "bound": "fp64-simt", "achieved": achieved, "unit": "TFLOP/s",
+                        "peak": None, "frac": None, "traffic": None,
+                        "note": "EMI runs on FP64 CUDA cores; algorithmic flops 2.7N^3+80N^2 per DS point"}
+        elif dom == "coherence":
+            q = N * (N - 1) // 2
+            mean_s = float(res.shp_num.float().mean().item())
+            flops = n_ds * (8 * mean_s * q + 3 * mean_s * N)
+            achieved = flops / (dom_ms / 1e3) / 1e12
+            roofline = {"kernel": "gram_kernel", "bound": "tensor", "achieved": achieved, "unit": "TFLOP/s",
+                        "peak": peaks.get("bf16_tflops"), "frac": achieved / peaks.get("bf16_tflops"),
+                        "traffic": None}
+        else:
+            npix = cfg.nlines * cfg.width
+            byts = npix * (4 * cfg.nimages + cfg.az_win * cfg.r_win + 4)
+            achieved = byts / (dom_ms / 1e3) / 1e9
+            roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "unit": "GB/s",
+                        "peak": peaks.get("hbm_gbs"), "frac": achieved / peaks.get("hbm_gbs"), "traffic": None}
+        roofline["peak_source"] = peaks["source"]
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        nthreads = len(os.sched_getaffinity(0))
+        side = min(args.cpu_sample, cfg.nlines)
+        sub = cfg.scaled(nlines=side, width=side,
+                         n_patches=max(4, cfg.n_patches * side * side // (cfg.nlines * cfg.width)))
+        z = make_stack(sub).numpy()
+        cpu_chain_rate(cfg, z[:48, :48], 48, nthreads)
+        r, dt, n = cpu_chain_rate(cfg, z, side, nthreads)
+        cpu = {"value": r, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": f"{side}x{side} crop of the scene model ({n} DS points, {dt:.1f} s), oracle chain"}
+
+    if rank == 0:
+        launches_per_step = 4 + 2 * max(1, -(-n_ds // chain.batch))
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32/c64 Gram, f64 EMI, u32 KS keys", "data": "synthetic",
+            "config": workload, "n_ds_per_gpu": n_ds, "stage_ms": stage, "roofline": roofline,
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches_per_step * args.steps,
+        }))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,160 @@
+/*
+ * moraine_b200 — C ABI of the B200 (sm_100a) distributed-scatterer chain.
+ *
+ * Every entry point takes DEVICE pointers to caller-allocated buffers, plain sizes and
+ * a CUDA stream (cudaStream_t passed as void*; NULL = legacy default stream). Work is
+ * enqueued on that stream and nothing synchronises the host, except where a function
+ * says so. Return value: MR_OK (0) or a negative MR_ERR_* code; mr_last_error() gives
+ * the message of the calling thread's last failure.
+ *
+ * Array layouts are those of the Python functions each entry point replaces (C order,
+ * numpy complex64 = interleaved float re, im):
+ *   rslc / rmli   (nlines, width, nimages)
+ *   p / dist      (nlines, width, az_win, r_win)         float32
+ *   is_shp        (nlines, width, az_win, r_win)         uint8 (numpy bool)
+ *   shp_num       (nlines, width)                        int32
+ *   idx           (n_pc, 2) int32, columns (azimuth, range)
+ *   pc_is_shp     (n_pc, az_win, r_win)                  uint8
+ *   coh           (n_pc, n_pairs) complex64, pairs in image_pairs order; image_pairs
+ *                 NULL means all pairs m < j in row-major upper-triangle order
+ *                 (numpy.triu_indices(nimages, 1)), n_pairs = nimages*(nimages-1)/2
+ *   ph            (n_pc, nimages) complex64
+ *
+ * Reference interfaces cited as path:line inside the kanglcn/moraine source tree.
+ */
+#ifndef MORAINE_B200_H
+#define MORAINE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* mr_stream_t; /* cudaStream_t */
+
+typedef struct {
+  float re, im;
+} mr_complex64;
+
+enum {
+  MR_OK = 0,
+  MR_ERR_INVALID = -1,     /* bad shape, size or argument */
+  MR_ERR_CUDA = -2,        /* a CUDA launch or API call failed */
+  MR_ERR_UNSUPPORTED = -3, /* valid request outside this build's limits */
+  MR_ERR_WORKSPACE = -4,   /* workspace missing or too small */
+};
+
+/* Arithmetic of the coherence Gram and of EMI. */
+enum {
+  MR_PREC_FP32 = 0,   /* FP32 SIMT Gram; EMI in FP64 */
+  MR_PREC_BF16 = 1,   /* BF16 tensor-core Gram, FP32 accumulate */
+  MR_PREC_BF16X3 = 2, /* BF16 hi/lo split tensor-core Gram (3 products) */
+  MR_PREC_FP64 = 3,   /* FP64 Gram */
+};
+
+/* Limits of this build. */
+#define MR_MAX_NIMAGES 512
+#define MR_MAX_WINDOW 4096 /* az_win * r_win */
+
+const char* mr_last_error(void);
+int mr_abi_version(void);
+
+/* ---------------------------------------------------------------- intensity prologue
+ * rmli = re*re + im*im (float32, each product and the sum rounded once): the |slc|^2
+ * that the notebooks feed to ks_test (nbs/API/pl.ipynb cell 15, `np.abs(rslc)**2`),
+ * written without a fused multiply-add. */
+int mr_intensity(const mr_complex64* rslc, int64_t n, float* rmli, mr_stream_t stream);
+
+/* ---------------------------------------------------------------- SHP identification
+ * Replaces moraine.shp.ks_test (moraine/shp.py:269-305) and, when is_shp / shp_num are
+ * given, moraine.shp.select_shp (moraine/shp.py:309-323) in the same pass.
+ * Two-sample KS test of every pixel against every pixel of its
+ * (2*az_half_win+1) x (2*r_half_win+1) window. The statistic is the exact integer
+ * k = max |j2 - j1| of the reference merge (moraine/shp.py:36-44); p and dist are
+ * float32 lookups of k through the reference formula evaluated on the host in double
+ * precision (moraine/shp.py:20-32, 74-76), so they equal the reference CPU path bit for
+ * bit; is_shp = (double)p < p_max and shp_num counts it. NaN (and is_shp = 0) where the
+ * neighbour is outside the image or either pixel holds a NaN.
+ * Any of p, dist, is_shp, shp_num may be NULL (is_shp and shp_num go together).
+ * workspace: >= mr_ks_workspace_bytes(), 16-byte aligned. */
+size_t mr_ks_workspace_bytes(int nlines, int width, int nimages);
+int mr_ks_test(const float* rmli, int nlines, int width, int nimages, int az_half_win,
+               int r_half_win, float* p, float* dist, double p_max, uint8_t* is_shp,
+               int32_t* shp_num, void* workspace, size_t workspace_bytes, mr_stream_t stream);
+
+/* Replaces moraine.shp.select_shp (moraine/shp.py:309-323): is_shp = p < p_max (p
+ * widened to double; NaN gives 0), shp_num = per-pixel count. */
+int mr_select_shp(const float* p, int64_t npix, int win, double p_max, uint8_t* is_shp,
+                  int32_t* shp_num, mr_stream_t stream);
+
+/* ---------------------------------------------------------------- DS candidates
+ * The glue the reference notebooks write between select_shp and emperical_co_pc
+ * (nbs/API/pl.ipynb cell 15: is_ds_can = shp_num >= 50; idx = stack(where(is_ds_can));
+ * pc_is_shp = is_shp[is_ds_can]), and the CLI's pc_logic_ras / ras2pc_ras_chunk
+ * (moraine/cli/pc.py:764, :239). Writes, in row-major pixel order, idx (n, 2) and,
+ * unless NULL, pc_is_shp (n, win); *n_ds (device int64) receives n. At most max_ds
+ * entries are written (n itself is always the full count).
+ * workspace: >= mr_ds_extract_workspace_bytes(). */
+size_t mr_ds_extract_workspace_bytes(int64_t npix);
+int mr_ds_extract(const int32_t* shp_num, const uint8_t* is_shp, int nlines, int width,
+                  int win, int min_shp, int32_t* idx, uint8_t* pc_is_shp, int64_t max_ds,
+                  int64_t* n_ds, void* workspace, size_t workspace_bytes, mr_stream_t stream);
+
+/* ---------------------------------------------------------------- coherence
+ * Replaces moraine.co.emperical_co_pc (moraine/co.py:230-266; kernel :141-190, CPU
+ * :194-227): coh[i, q] = sum_s z_m conj(z_j) / sqrt(sum_s |z_m|^2 * sum_s |z_j|^2) over
+ * the SHPs s of point i that lie inside the image, (m, j) = image_pairs[q].
+ * mask_stride selects where each point's window mask lives: mask_stride == 0 reads
+ * pc_is_shp (n_pc, az_win, r_win); mask_stride == 1 reads a raster is_shp
+ * (nlines, width, az_win, r_win) at the point's own pixel (the chain's layout).
+ * precision: MR_PREC_FP32, MR_PREC_BF16, MR_PREC_BF16X3 or MR_PREC_FP64 (custom
+ * image_pairs: FP32 only). */
+int mr_emperical_co_pc(const mr_complex64* rslc, int nlines, int width, int nimages,
+                       const int32_t* idx, int64_t n_pc, const uint8_t* mask, int mask_stride,
+                       int az_win, int r_win, const int32_t* image_pairs, int n_pairs,
+                       mr_complex64* coh, int precision, mr_stream_t stream);
+
+/* Replaces moraine.co.emperical_co (moraine/co.py:117-137; kernel :61-114): full
+ * (nlines, width, nimages, nimages) covariance cov = sum/n_shp and coherence. */
+int mr_emperical_co(const mr_complex64* rslc, int nlines, int width, int nimages,
+                    const uint8_t* is_shp, int az_win, int r_win, mr_complex64* cov,
+                    mr_complex64* coh, mr_stream_t stream);
+
+/* Replaces moraine.co.uncompress_coh (moraine/co.py:281-299): (n, n_pairs) ->
+ * (n, nimages, nimages) Hermitian, zero where no pair is given, unit diagonal. */
+int mr_uncompress_coh(const mr_complex64* coh, int64_t n, int nimages,
+                      const int32_t* image_pairs, int n_pairs, mr_complex64* out,
+                      mr_stream_t stream);
+
+/* ---------------------------------------------------------------- phase linking
+ * Replaces moraine.pl.emi (moraine/pl.py:68-77; GPU :19-42, CPU :46-65): for every
+ * point, M = inv(|Gamma|) o Gamma from the full-triangle compressed coherence, its
+ * algebraically smallest eigenpair (lambda, v), ph = v conj(v[ref]) / |v conj(v[ref])|,
+ * emi_quality = lambda. inv(|Gamma|) by pivoted Gauss-Jordan, eigenpair by Householder
+ * tridiagonalisation, Sturm bisection and inverse iteration, all in FP64.
+ * t_coh (may be NULL) receives moraine.pl.ds_temp_coh of the result (moraine/pl.py:126)
+ * computed in the same pass. workspace: >= mr_emi_workspace_bytes(). */
+size_t mr_emi_workspace_bytes(int64_t n_pc, int nimages);
+int mr_emi(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, mr_complex64* ph,
+           float* emi_quality, float* t_coh, void* workspace, size_t workspace_bytes,
+           mr_stream_t stream);
+
+/* ---------------------------------------------------------------- temporal coherence
+ * Replaces moraine.pl.ds_temp_coh (moraine/pl.py:126-145; kernel :104-123):
+ * t = |sum_q coh_q/|coh_q| conj(ph_m) ph_j| / n_pairs. */
+int mr_ds_temp_coh(const mr_complex64* coh, const mr_complex64* ph, int64_t n, int nimages,
+                   const int32_t* image_pairs, int n_pairs, float* t_coh, mr_stream_t stream);
+
+/* Replaces moraine.pqm.temp_coh (moraine/pqm.py:124-159; kernel :100-121):
+ * t = |sum_q intf_q conj(r_m) r_j / sqrt(|intf_q|^2 |r_m|^2 |r_j|^2)| / n_pairs.
+ * Inputs are not modified (the reference CPU path normalises them in place). */
+int mr_temp_coh(const mr_complex64* intf, const mr_complex64* rslc, int64_t n, int nimages,
+                const int32_t* image_pairs, int n_pairs, float* t_coh, mr_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MORAINE_B200_H */

@@ -1,0 +1,107 @@
+"""The distributed-scatterer chain on one device: the production caller of the kernels.
+
+Replaces the reference's file-based stage drivers (moraine/cli/shp.py:33-123,
+moraine/cli/co.py:33-157, moraine/cli/pl.py:223-361) for one tile resident in HBM:
+
+    rslc -> intensity -> KS test + selection -> DS candidates
+         -> [coherence -> EMI (+ temporal coherence)] per batch of DS points
+
+Every intermediate (intensity, sort keys, SHP masks, counts, DS indices, coherence of
+the current batch) stays on the device; buffers are allocated once per plan and reused.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _dev, _lib
+
+
+@dataclass
+class ChainResult:
+    n_ds: int
+    idx: torch.Tensor          # (n_ds, 2) int32
+    ph: torch.Tensor           # (n_ds, N) complex64
+    quality: torch.Tensor      # (n_ds,) float32
+    t_coh: torch.Tensor        # (n_ds,) float32
+    shp_num: torch.Tensor      # (nlines, width) int32
+    is_shp: torch.Tensor       # (nlines, width, az_win, r_win) uint8
+    stage_ms: dict = field(default_factory=dict)
+
+
+class DsChain:
+    """Plan and buffers for one (nlines, width, nimages, window) shape."""
+
+    def __init__(self, nlines: int, width: int, nimages: int, az_half_win: int, r_half_win: int,
+                 p_max: float = 0.05, min_shp: int = 50, precision: str = "fp32", batch: int | None = None,
+                 device=None, timing: bool = False):
+        self.device = torch.device(device) if device is not None else _dev.require_cuda()
+        self.shape = (nlines, width, nimages)
+        self.azh, self.rh = az_half_win, r_half_win
+        self.az_win, self.r_win = 2 * az_half_win + 1, 2 * r_half_win + 1
+        self.win = self.az_win * self.r_win
+        self.p_max, self.min_shp = float(p_max), int(min_shp)
+        self.prec = _lib.PREC[precision]
+        self.timing = timing
+        self.npairs = nimages * (nimages - 1) // 2
+        npix = nlines * width
+        if batch is None:
+            batch = max(1024, min(npix, (8 << 30) // (8 * self.npairs)))  # <= 8 GiB coherence per batch
+        self.batch = int(batch)
+        lib = _lib.load()
+        d = self.device
+        self.rmli = torch.empty((nlines, width, nimages), dtype=torch.float32, device=d)
+        self.ks_ws = _dev.workspace(lib.mr_ks_workspace_bytes(nlines, width, nimages), d)
+        self.is_shp = torch.empty((nlines, width, self.az_win, self.r_win), dtype=torch.uint8, device=d)
+        self.shp_num = torch.empty((nlines, width), dtype=torch.int32, device=d)
+        self.ex_ws = _dev.workspace(lib.mr_ds_extract_workspace_bytes(npix), d)
+        self.idx = torch.empty((npix, 2), dtype=torch.int32, device=d)
+        self.n_ds_dev = torch.zeros((1,), dtype=torch.int64, device=d)
+        self.coh = torch.empty((self.batch, self.npairs), dtype=torch.complex64, device=d)
+        self.emi_ws = _dev.workspace(lib.mr_emi_workspace_bytes(self.batch, nimages), d)
+        self.ph = torch.empty((npix, nimages), dtype=torch.complex64, device=d)
+        self.quality = torch.empty((npix,), dtype=torch.float32, device=d)
+        self.t_coh = torch.empty((npix,), dtype=torch.float32, device=d)
+
+    def run(self, rslc: torch.Tensor) -> ChainResult:
+        nlines, width, n = self.shape
+        assert rslc.shape == self.shape and rslc.dtype == torch.complex64 and rslc.is_cuda
+        rslc = rslc.contiguous()
+        s = _dev.stream()
+        ev = []
+
+        def mark(name):
+            if self.timing:
+                e = torch.cuda.Event(enable_timing=True)
+                e.record()
+                ev.append((name, e))
+
+        mark("start")
+        _lib.call("mr_intensity", rslc.data_ptr(), rslc.numel(), self.rmli.data_ptr(), s)
+        mark("intensity")
+        _lib.call("mr_ks_test", self.rmli.data_ptr(), nlines, width, n, self.azh, self.rh, None, None, self.p_max,
+                  self.is_shp.data_ptr(), self.shp_num.data_ptr(), self.ks_ws.data_ptr(), self.ks_ws.numel(), s)
+        mark("ks_select")
+        npix = nlines * width
+        _lib.call("mr_ds_extract", self.shp_num.data_ptr(), None, nlines, width, self.win, self.min_shp,
+                  self.idx.data_ptr(), None, npix, self.n_ds_dev.data_ptr(), self.ex_ws.data_ptr(),
+                  self.ex_ws.numel(), s)
+        mark("extract")
+        n_ds = int(self.n_ds_dev.item())
+        for b0 in range(0, n_ds, self.batch):
+            nb = min(self.batch, n_ds - b0)
+            _lib.call("mr_emperical_co_pc", rslc.data_ptr(), nlines, width, n, self.idx[b0].data_ptr(), nb,
+                      self.is_shp.data_ptr(), 1, self.az_win, self.r_win, None, self.npairs, self.coh.data_ptr(),
+                      self.prec, s)
+            mark("coherence")
+            _lib.call("mr_emi", self.coh.data_ptr(), nb, n, 0, self.ph[b0].data_ptr(), self.quality[b0:].data_ptr(),
+                      self.t_coh[b0:].data_ptr(), self.emi_ws.data_ptr(), self.emi_ws.numel(), s)
+            mark("emi_tcoh")
+        stage = {}
+        if self.timing:
+            torch.cuda.synchronize()
+            for (_, a), (name, b) in zip(ev[:-1], ev[1:]):
+                stage[name] = stage.get(name, 0.0) + a.elapsed_time(b)
+        return ChainResult(n_ds, self.idx[:n_ds], self.ph[:n_ds], self.quality[:n_ds], self.t_coh[:n_ds],
+                           self.shp_num, self.is_shp, stage)

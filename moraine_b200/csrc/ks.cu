@@ -1,0 +1,368 @@
+// SHP identification: per-pixel sort to order-preserving keys, then the two-sample
+// Kolmogorov-Smirnov merge of every pixel against its window, with the selection
+// (p < p_max, per-pixel count) fused into the epilogue.
+//
+// Reference behaviour followed (kanglcn/moraine):
+//   moraine/shp.py:36-44    merge: ties advance both indices, D*N = max |j2 - j1|
+//   moraine/shp.py:20-32    p = sum_{i<=100} (-1)^(i-1) 2 exp(-2 i^2 x^2), early exit p == p_prev
+//   moraine/shp.py:74-76    x = (sqrt(N/2) + 0.12 + 0.11/sqrt(N/2)) * D, p stored as float32
+//   moraine/shp.py:58-72    NaN outside the image or when either pixel's last sorted value is NaN
+//   moraine/shp.py:309-323  is_shp = p < p_max (float32 p against a double p_max), count
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mr {
+namespace {
+
+constexpr uint32_t kKeyMax = 0xFFFFFFFFu;  // NaN key and merge sentinel
+
+// Order-preserving map float -> uint32: -0 and +0 share a key (they compare equal in the
+// reference merge), NaN maps above +inf (numpy.sort puts NaN last).
+__device__ __forceinline__ uint32_t float_key(float f) {
+  if (isnan(f)) return kKeyMax;
+  uint32_t b = __float_as_uint(f);
+  if (b == 0x80000000u) b = 0u;
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+// Global key stride of one pixel: nimages keys, then sentinels, padded to 16 bytes.
+__host__ __device__ __forceinline__ int key_stride(int n) { return (n + 1 + 3) & ~3; }
+
+// ------------------------------------------------------------------------- sort
+// One warp per pixel, E keys per lane in the layout i = r*32 + lane; bitonic network
+// over 32*E keys (padding keys are kKeyMax and sort last).
+template <int E>
+__global__ void __launch_bounds__(256) sort_keys_kernel(const float* __restrict__ rmli,
+                                                        int64_t npix, int n,
+                                                        uint32_t* __restrict__ keys) {
+  constexpr int NP = 32 * E;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps_total = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int ks = key_stride(n);
+  for (int64_t pix = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); pix < npix;
+       pix += warps_total) {
+    uint32_t v[E];
+    const float* src = rmli + pix * n;
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      int i = r * 32 + lane;
+      v[r] = (i < n) ? float_key(__ldg(src + i)) : kKeyMax;
+    }
+#pragma unroll
+    for (int k = 2; k <= NP; k <<= 1) {
+#pragma unroll
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        if (j >= 32) {
+          const int rj = j >> 5;
+#pragma unroll
+          for (int r = 0; r < E; ++r) {
+            if ((r & rj) == 0) {
+              const int i = r * 32 + lane;
+              const bool up = (i & k) == 0;
+              uint32_t a = v[r], b = v[r ^ rj];
+              if (up ? (a > b) : (a < b)) { v[r] = b; v[r ^ rj] = a; }
+            }
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < E; ++r) {
+            const int i = r * 32 + lane;
+            const bool up = (i & k) == 0;
+            const bool lower = (lane & j) == 0;
+            uint32_t o = __shfl_xor_sync(0xffffffffu, v[r], j);
+            uint32_t mn = min(v[r], o), mx = max(v[r], o);
+            v[r] = (up == lower) ? mn : mx;
+          }
+        }
+      }
+    }
+    uint32_t* dst = keys + pix * ks;
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      int i = r * 32 + lane;
+      if (i < ks) dst[i] = (i < n) ? v[r] : kKeyMax;
+    }
+    for (int i = NP + lane; i < ks; i += 32) dst[i] = kKeyMax;
+  }
+}
+
+// ------------------------------------------------------------------------- KS merge
+struct KsTable {
+  float p[MR_MAX_NIMAGES + 1];
+  float dist[MR_MAX_NIMAGES + 1];
+  uint8_t accept[MR_MAX_NIMAGES + 1];
+};
+
+struct KsPlan {
+  int th, tw, azc;  // output tile rows/cols, azimuth window offsets per chunk
+  int ss;           // shared-memory words per pixel (odd: conflict-free across lanes)
+  size_t smem;
+};
+
+constexpr int kKsThreads = 256;
+
+__global__ void __launch_bounds__(kKsThreads) ks_merge_kernel(
+    const uint32_t* __restrict__ keys, int nlines, int width, int n, int azh, int rh,
+    int th, int tw, int azc, int ss, const __grid_constant__ KsTable tab, float* __restrict__ p,
+    float* __restrict__ dist, uint8_t* __restrict__ is_shp, int32_t* __restrict__ shp_num) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  const int az_win = 2 * azh + 1, r_win = 2 * rh + 1, win = az_win * r_win;
+  const int nrp = th * tw;
+  const int hw = tw + 2 * rh;  // halo width
+  uint32_t* ref_tile = smem;                      // nrp pixels
+  uint32_t* halo = smem + (size_t)nrp * ss;       // (th + azc - 1) x hw pixels
+  __shared__ float s_p[MR_MAX_NIMAGES + 1];
+  __shared__ float s_d[MR_MAX_NIMAGES + 1];
+  __shared__ uint8_t s_acc[MR_MAX_NIMAGES + 1];
+  __shared__ int s_cnt[kKsThreads];
+  __shared__ uint8_t s_nan_ref[kKsThreads];
+
+  for (int k = threadIdx.x; k <= n; k += blockDim.x) {
+    s_p[k] = tab.p[k];
+    s_d[k] = tab.dist[k];
+    s_acc[k] = tab.accept[k];
+  }
+  const int ks = key_stride(n);
+  const int tiles_x = (width + tw - 1) / tw;
+  const int r0 = (blockIdx.x / tiles_x) * th;
+  const int c0 = (blockIdx.x % tiles_x) * tw;
+
+  // reference tile
+  for (int e = threadIdx.x; e < nrp * ks; e += blockDim.x) {
+    int rp = e / ks, i = e - rp * ks;
+    int r = r0 + rp / tw, c = c0 + rp % tw;
+    uint32_t v = kKeyMax;
+    if (r < nlines && c < width) v = keys[((int64_t)r * width + c) * ks + i];
+    if (i <= n) ref_tile[rp * ss + i] = v;
+  }
+  if (threadIdx.x < nrp) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
+  if (threadIdx.x < nrp) s_nan_ref[threadIdx.x] = (ref_tile[threadIdx.x * ss + n - 1] == kKeyMax);
+
+  const int rp = threadIdx.x % nrp;
+  const int slot = threadIdx.x / nrp, nslots = blockDim.x / nrp;
+  const int rr = r0 + rp / tw, rc = c0 + rp % tw;
+  const bool ref_in = (rr < nlines) && (rc < width);
+  int count = 0;
+
+  for (int z0 = 0; z0 < az_win; z0 += azc) {
+    const int nz = min(azc, az_win - z0);
+    const int hrows = th + nz - 1;
+    __syncthreads();  // previous chunk done with the halo
+    // halo rows: image rows r0 - azh + z0 .. + hrows-1, cols c0 - rh .. + hw-1
+    for (int e = threadIdx.x; e < hrows * hw * ks; e += blockDim.x) {
+      int hp = e / ks, i = e - hp * ks;
+      int r = r0 - azh + z0 + hp / hw, c = c0 - rh + hp % hw;
+      uint32_t v = kKeyMax;
+      if (r >= 0 && r < nlines && c >= 0 && c < width) v = keys[((int64_t)r * width + c) * ks + i];
+      if (i <= n) halo[hp * ss + i] = v;
+    }
+    __syncthreads();
+    if (ref_in) {
+      const uint32_t* A = ref_tile + rp * ss;
+      const bool nan_ref = s_nan_ref[rp];
+      for (int o = slot; o < nz * r_win; o += nslots) {
+        const int oz = o / r_win, orr = o - oz * r_win;
+        const int sr = rr - azh + z0 + oz, sc = rc - rh + orr;
+        const int64_t out = ((int64_t)rr * width + rc) * win + (int64_t)(z0 + oz) * r_win + orr;
+        float pv = __int_as_float(0x7fffffff), dv = pv;
+        uint8_t acc = 0;
+        if (sr >= 0 && sr < nlines && sc >= 0 && sc < width && !nan_ref) {
+          const uint32_t* B = halo + ((rp / tw + oz) * hw + (rp % tw + orr)) * ss;
+          if (B[n - 1] != kKeyMax) {
+            uint32_t a = A[0], b = B[0];
+            int j1 = 0, j2 = 0, kmax = 0;
+            while (j1 < n && j2 < n) {
+              const int le = a <= b, ge = a >= b;
+              j1 += le;
+              j2 += ge;
+              a = A[j1];
+              b = B[j2];
+              kmax = max(kmax, abs(j2 - j1));
+            }
+            pv = s_p[kmax];
+            dv = s_d[kmax];
+            acc = s_acc[kmax];
+          }
+        }
+        if (p) p[out] = pv;
+        if (dist) dist[out] = dv;
+        if (is_shp) is_shp[out] = acc;
+        count += acc;
+      }
+    }
+  }
+  if (shp_num) {
+    if (ref_in && count) atomicAdd(&s_cnt[rp], count);
+    __syncthreads();
+    if (threadIdx.x < nrp) {
+      int r = r0 + threadIdx.x / tw, c = c0 + threadIdx.x % tw;
+      if (r < nlines && c < width) shp_num[(int64_t)r * width + c] = s_cnt[threadIdx.x];
+    }
+  }
+}
+
+// The reference p formula (moraine/shp.py:20-32) evaluated in double with the same
+// operation order, no contraction; stored as float32 like the reference's output array.
+double ks_p_reference(double x) {
+  const double x2 = -2.0 * x * x;
+  double p = 0.0, p2 = 0.0;
+  int sign = 1;
+  for (int i = 1; i <= 100; ++i) {
+    p += (double)(sign * 2) * std::exp(x2 * (double)i * (double)i);
+    if (p == p2) return p;
+    sign = -sign;
+    p2 = p;
+  }
+  return p;
+}
+
+void fill_table(KsTable& t, int n, double p_max) {
+  const double en = std::sqrt((double)n / 2.0);
+  const double scale = en + 0.12 + 0.11 / en;
+  for (int k = 0; k <= n; ++k) {
+    const double d = std::fabs((double)k / (double)n);
+    const float pf = (float)ks_p_reference(scale * d);
+    t.p[k] = pf;
+    t.dist[k] = (float)d;
+    t.accept[k] = ((double)pf < p_max) ? 1 : 0;
+  }
+}
+
+KsPlan plan_ks(int n, int azh, int rh) {
+  const int az_win = 2 * azh + 1;
+  KsPlan best{0, 0, 0, (n + 1) | 1, 0};
+  const size_t budget = 200 * 1024;
+  double best_score = -1;
+  const int tws[] = {32, 16, 8, 4, 2, 1};
+  for (int tw : tws) {
+    for (int th = 1; th * tw <= kKsThreads; th *= 2) {
+      if (kKsThreads % (th * tw)) continue;
+      for (int azc = az_win; azc >= 1; --azc) {
+        size_t px = (size_t)th * tw + (size_t)(th + azc - 1) * (tw + 2 * rh);
+        size_t bytes = px * best.ss * 4;
+        if (bytes > budget) continue;
+        // merges per loaded pixel, preferring full warps of reference pixels
+        int nchunks = (az_win + azc - 1) / azc;
+        double loaded = (double)th * tw + (double)nchunks * (th + azc - 1) * (tw + 2 * rh);
+        double score = (double)th * tw / loaded * (th * tw >= 32 ? 1.0 : 0.5);
+        if (score > best_score) {
+          best_score = score;
+          best.th = th; best.tw = tw; best.azc = azc; best.smem = bytes;
+        }
+        break;  // largest fitting azc for this (tw, th)
+      }
+    }
+  }
+  return best;
+}
+
+// ------------------------------------------------------------------------- misc
+__global__ void intensity_kernel(const float2* __restrict__ z, int64_t n, float* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float2 v = z[i];
+    out[i] = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
+  }
+}
+
+// One warp per pixel: is_shp = (double)p < p_max, shp_num = count.
+__global__ void select_shp_kernel(const float* __restrict__ p, int64_t npix, int win, double p_max,
+                                  uint8_t* __restrict__ is_shp, int32_t* __restrict__ shp_num) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t pix = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); pix < npix; pix += nw) {
+    int cnt = 0;
+    for (int o = lane; o < win; o += 32) {
+      const int64_t e = pix * win + o;
+      const uint8_t s = ((double)p[e] < p_max) ? 1 : 0;
+      if (is_shp) is_shp[e] = s;
+      cnt += s;
+    }
+    cnt = warp_sum(cnt);
+    if (lane == 0 && shp_num) shp_num[pix] = cnt;
+  }
+}
+
+template <int E>
+void launch_sort(const float* rmli, int64_t npix, int n, uint32_t* keys, cudaStream_t s) {
+  int64_t blocks = (npix + 7) / 8;
+  int grid = (int)std::min<int64_t>(blocks, (int64_t)sm_count() * 32);
+  sort_keys_kernel<E><<<grid, 256, 0, s>>>(rmli, npix, n, keys);
+}
+
+}  // namespace
+}  // namespace mr
+
+using namespace mr;
+
+extern "C" size_t mr_ks_workspace_bytes(int nlines, int width, int nimages) {
+  if (nlines <= 0 || width <= 0 || nimages <= 0) return 0;
+  return (size_t)nlines * width * key_stride(nimages) * sizeof(uint32_t);
+}
+
+extern "C" int mr_ks_test(const float* rmli, int nlines, int width, int nimages, int az_half_win,
+                          int r_half_win, float* p, float* dist, double p_max, uint8_t* is_shp,
+                          int32_t* shp_num, void* workspace, size_t workspace_bytes,
+                          mr_stream_t stream) {
+  MR_REQUIRE(rmli != nullptr, "ks_test: rmli is NULL");
+  MR_REQUIRE(nlines > 0 && width > 0, "ks_test: empty image (%d x %d)", nlines, width);
+  MR_REQUIRE(nimages >= 1, "ks_test: nimages must be >= 1 (got %d)", nimages);
+  if (nimages > MR_MAX_NIMAGES)
+    return fail(MR_ERR_UNSUPPORTED, "ks_test: nimages %d > %d", nimages, MR_MAX_NIMAGES);
+  MR_REQUIRE(az_half_win >= 0 && r_half_win >= 0, "ks_test: negative half window");
+  const int64_t win = (int64_t)(2 * az_half_win + 1) * (2 * r_half_win + 1);
+  if (win > MR_MAX_WINDOW) return fail(MR_ERR_UNSUPPORTED, "ks_test: window %lld > %d", (long long)win, MR_MAX_WINDOW);
+  MR_REQUIRE((is_shp == nullptr) == (shp_num == nullptr), "ks_test: is_shp and shp_num go together");
+  const size_t need = mr_ks_workspace_bytes(nlines, width, nimages);
+  if (workspace == nullptr || workspace_bytes < need)
+    return fail(MR_ERR_WORKSPACE, "ks_test: workspace %zu < %zu bytes", workspace_bytes, need);
+  MR_REQUIRE(((uintptr_t)workspace & 15) == 0, "ks_test: workspace not 16-byte aligned");
+  cudaStream_t s = as_stream(stream);
+  const int64_t npix = (int64_t)nlines * width;
+  uint32_t* keys = static_cast<uint32_t*>(workspace);
+  if (nimages <= 32) launch_sort<1>(rmli, npix, nimages, keys, s);
+  else if (nimages <= 64) launch_sort<2>(rmli, npix, nimages, keys, s);
+  else if (nimages <= 128) launch_sort<4>(rmli, npix, nimages, keys, s);
+  else if (nimages <= 256) launch_sort<8>(rmli, npix, nimages, keys, s);
+  else launch_sort<16>(rmli, npix, nimages, keys, s);
+  if (int rc = check_launch("ks_test sort")) return rc;
+  if (!p && !dist && !is_shp) return MR_OK;
+
+  KsPlan plan = plan_ks(nimages, az_half_win, r_half_win);
+  if (plan.th == 0)
+    return fail(MR_ERR_UNSUPPORTED, "ks_test: nimages %d with half windows (%d, %d) does not fit shared memory",
+                nimages, az_half_win, r_half_win);
+  // host staging of the table; the launch copies it into the kernel's parameter buffer
+  static thread_local KsTable tab_local;
+  fill_table(tab_local, nimages, p_max);
+  MR_CUDA_TRY(cudaFuncSetAttribute(ks_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)plan.smem));
+  const int64_t tiles = (int64_t)((nlines + plan.th - 1) / plan.th) * ((width + plan.tw - 1) / plan.tw);
+  MR_REQUIRE(tiles < (1ll << 31), "ks_test: image too large");
+  ks_merge_kernel<<<(unsigned)tiles, kKsThreads, plan.smem, s>>>(
+      keys, nlines, width, nimages, az_half_win, r_half_win, plan.th, plan.tw, plan.azc, plan.ss,
+      tab_local, p, dist, is_shp, shp_num);
+  return check_launch("ks_test merge");
+}
+
+extern "C" int mr_select_shp(const float* p, int64_t npix, int win, double p_max, uint8_t* is_shp,
+                             int32_t* shp_num, mr_stream_t stream) {
+  MR_REQUIRE(p != nullptr, "select_shp: p is NULL");
+  MR_REQUIRE(npix >= 0 && win > 0, "select_shp: bad shape");
+  if (npix == 0) return MR_OK;
+  int64_t blocks = (npix + 7) / 8;
+  int grid = (int)std::min<int64_t>(blocks, (int64_t)sm_count() * 16);
+  select_shp_kernel<<<grid, 256, 0, as_stream(stream)>>>(p, npix, win, p_max, is_shp, shp_num);
+  return check_launch("select_shp");
+}
+
+extern "C" int mr_intensity(const mr_complex64* rslc, int64_t n, float* rmli, mr_stream_t stream) {
+  MR_REQUIRE(rslc && rmli, "intensity: NULL pointer");
+  if (n <= 0) return MR_OK;
+  int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 16);
+  intensity_kernel<<<grid, 256, 0, as_stream(stream)>>>(reinterpret_cast<const float2*>(rslc), n, rmli);
+  return check_launch("intensity");
+}

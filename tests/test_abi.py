@@ -1,0 +1,52 @@
+"""The C-ABI library loads, exports every declared symbol, and validates on the host."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from moraine_b200 import _lib
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "moraine_b200.h"
+
+
+def declared():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(mr_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = declared()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(lib, n), n
+    assert sorted(_lib.exported_symbols()) == names
+
+
+def test_version_and_sizes():
+    lib = _lib.load()
+    assert lib.mr_abi_version() == 1
+    assert lib.mr_ks_workspace_bytes(200, 200, 17) == 200 * 200 * 20 * 4
+    assert lib.mr_ks_workspace_bytes(0, 200, 17) == 0
+    assert lib.mr_ds_extract_workspace_bytes(4096) == 4 * 8
+
+
+@pytest.mark.parametrize("call,code", [
+    (lambda L: L.mr_ks_test(None, 10, 10, 17, 1, 1, None, None, 0.05, None, None, None, 0, None), _lib.MR_ERR_INVALID),
+    (lambda L: L.mr_ks_test(16, 10, 10, 600, 1, 1, None, None, 0.05, None, None, 16, 10**9, None),
+     _lib.MR_ERR_UNSUPPORTED),
+    (lambda L: L.mr_ks_test(16, 10, 10, 17, 1, 1, 16, None, 0.05, None, None, 16, 10, None), _lib.MR_ERR_WORKSPACE),
+    (lambda L: L.mr_ks_test(16, 10, 10, 17, 1, 1, 16, None, 0.05, 16, None, 16, 10**9, None), _lib.MR_ERR_INVALID),
+    (lambda L: L.mr_emi(16, 10, 17, 17, 16, 16, None, 16, 10**9, None), _lib.MR_ERR_INVALID),
+    (lambda L: L.mr_emi(16, 10, 1, 0, 16, 16, None, 16, 10**9, None), _lib.MR_ERR_INVALID),
+    (lambda L: L.mr_emperical_co_pc(16, 10, 10, 17, 16, 5, 16, 0, 4, 3, None, 0, 16, 0, None), _lib.MR_ERR_INVALID),
+    (lambda L: L.mr_emperical_co_pc(16, 10, 10, 17, 16, 5, 16, 2, 3, 3, None, 0, 16, 0, None), _lib.MR_ERR_INVALID),
+    (lambda L: L.mr_ds_extract(16, None, 10, 10, 9, 3, 16, 16, 100, 16, 16, 10**6, None), _lib.MR_ERR_INVALID),
+])
+def test_host_validation_without_gpu(call, code):
+    """Bad arguments are rejected before any device work (these calls never launch)."""
+    lib = _lib.load()
+    assert call(lib) == code
+    assert _lib.last_error()

@@ -1,0 +1,236 @@
+"""Parity of the CUDA path (through the C ABI) with the reference fixtures and the oracle."""
+import numpy as np
+import pytest
+import torch
+
+import moraine_b200 as mb
+from moraine_b200.chain import DsChain
+from moraine_b200.synth import CONFIGS, make_stack
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+EPS32, EPS64 = 6e-8, 1.2e-16
+
+
+# ----------------------------------------------------------------------------- KS
+@pytest.mark.parametrize("tag", ["a", "b", "c"])
+def test_ks_matches_reference_fixture(cuda, golden, tag):
+    g = golden("ks_small.npz")
+    x, (azh, rh) = g[f"{tag}_rmli"], (int(v) for v in g[f"{tag}_win"])
+    p = mb.ks_test(x, azh, rh)
+    np.testing.assert_array_equal(p, g[f"{tag}_p"])
+    dist, pd = mb.ks_test(x, azh, rh, return_dist=True)
+    np.testing.assert_array_equal(pd, g[f"{tag}_pd"])
+    ok = ~np.isnan(g[f"{tag}_p"])
+    np.testing.assert_array_equal(dist[ok], g[f"{tag}_dist"][ok])
+    is_shp, shp_num = mb.select_shp(p, 0.05)
+    np.testing.assert_array_equal(is_shp, g[f"{tag}_is_shp"])
+    np.testing.assert_array_equal(shp_num, g[f"{tag}_shp_num"])
+
+
+def _fused_select(rmli_t, azh, rh, p_max=0.05):
+    from moraine_b200 import _dev, _lib
+    nl, w, n = rmli_t.shape
+    win = (2 * azh + 1) * (2 * rh + 1)
+    is_shp = torch.empty((nl, w, win), dtype=torch.uint8, device=rmli_t.device)
+    num = torch.empty((nl, w), dtype=torch.int32, device=rmli_t.device)
+    p = torch.empty((nl, w, win), dtype=torch.float32, device=rmli_t.device)
+    ws = _dev.workspace(_lib.load().mr_ks_workspace_bytes(nl, w, n), rmli_t.device)
+    _lib.call("mr_ks_test", rmli_t.data_ptr(), nl, w, n, azh, rh, p.data_ptr(), None, p_max, is_shp.data_ptr(),
+              num.data_ptr(), ws.data_ptr(), ws.numel(), _dev.stream())
+    return p.cpu().numpy(), is_shp.cpu().numpy().astype(bool), num.cpu().numpy()
+
+
+@pytest.mark.parametrize("name,size", [("c0", 200), ("c1", 72), ("c2", 64), ("c3", 40)])
+def test_ks_bit_exact_vs_oracle(cuda, name, size):
+    """Bit-exact p, mask and counts at the configs' image counts and windows."""
+    cfg = CONFIGS[name].scaled(nlines=size, width=size + 3)
+    z = make_stack(cfg)
+    rmli = O.intensity(z.numpy())
+    p_ref = O.ks_test(rmli, cfg.az_half_win, cfg.r_half_win)
+    is_ref, num_ref = O.select_shp(p_ref, cfg.p_max)
+    p, is_shp, num = _fused_select(torch.from_numpy(rmli).to(cuda), cfg.az_half_win, cfg.r_half_win, cfg.p_max)
+    np.testing.assert_array_equal(p.reshape(p_ref.shape), p_ref)
+    np.testing.assert_array_equal(is_shp.reshape(is_ref.shape), is_ref)
+    np.testing.assert_array_equal(num, num_ref)
+
+
+def test_ks_edges(cuda):
+    rng = np.random.default_rng(0)
+    # window larger than the image, N = 1 and N = 2, NaN everywhere
+    for (nl, w, n, azh, rh) in [(3, 4, 6, 5, 7), (5, 5, 1, 1, 1), (6, 7, 2, 2, 2), (1, 9, 33, 0, 4), (9, 1, 65, 3, 0)]:
+        x = rng.exponential(size=(nl, w, n)).astype(np.float32)
+        x[0, 0, 0] = np.nan
+        np.testing.assert_array_equal(mb.ks_test(x, azh, rh), O.ks_test(x, azh, rh))
+    x = np.full((4, 4, 8), np.nan, np.float32)
+    assert np.isnan(mb.ks_test(x, 1, 1)).all()
+
+
+# ----------------------------------------------------------------------------- coherence
+def test_co_pc_matches_reference_fixture(cuda, golden):
+    g = golden("co_small.npz")
+    coh = mb.emperical_co_pc(g["rslc"], g["idx"], g["pc_is_shp"])
+    np.testing.assert_allclose(coh, g["coh"], atol=1e-6, rtol=0)
+    coh_bw = mb.emperical_co_pc(g["rslc"], g["idx"], g["pc_is_shp"], image_pairs=g["pairs_bw"])
+    np.testing.assert_allclose(coh_bw, g["coh_bw"], atol=1e-6, rtol=0)
+    np.testing.assert_array_equal(mb.uncompress_coh(g["coh_bw"], g["pairs_bw"]), g["unc_bw"])
+    np.testing.assert_array_equal(mb.uncompress_coh(g["coh"]), O.uncompress_coh(g["coh"]))
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", 2e-6), ("fp64", 1e-7)])
+@pytest.mark.parametrize("name,size", [("c0", 64), ("c1", 48), ("c2", 48), ("c3", 24)])
+def test_co_pc_vs_oracle(cuda, name, size, precision, tol):
+    cfg = CONFIGS[name].scaled(nlines=size, width=size)
+    z = make_stack(cfg).numpy()
+    p = O.ks_test(O.intensity(z), cfg.az_half_win, cfg.r_half_win)
+    is_shp, num = O.select_shp(p, cfg.p_max)
+    idx, pc = O.ds_candidates(is_shp, num, 1)
+    ref = O.emperical_co_pc(z, idx, pc)
+    coh = mb.emperical_co_pc(z, idx, pc, precision=precision)
+    assert np.abs(coh - ref).max() < tol
+
+
+def test_co_raster_vs_oracle(cuda):
+    rng = np.random.default_rng(4)
+    z = (rng.standard_normal((9, 13, 7)) + 1j * rng.standard_normal((9, 13, 7))).astype(np.complex64)
+    m = rng.random((9, 13, 3, 5)) < 0.6
+    m[:, :, 1, 2] = True
+    cov, coh = mb.emperical_co(z, m)
+    cov_r, coh_r = O.emperical_co(z, m)
+    np.testing.assert_allclose(cov, cov_r, atol=2e-6, rtol=1e-5)
+    np.testing.assert_allclose(coh, coh_r, atol=2e-6)
+    sel = np.count_nonzero(m, axis=(-2, -1)) >= 3
+    idx = np.stack(np.where(sel), -1)
+    r, s = np.triu_indices(7, 1)
+    np.testing.assert_allclose(coh[sel][:, r, s], mb.emperical_co_pc(z, idx, m[sel]), atol=1e-6)
+
+
+# ----------------------------------------------------------------------------- EMI, temporal coherence
+def test_emi_vs_reference_fixture(cuda, golden):
+    g = golden("co_small.npz")
+    ph, q = mb.emi(g["coh"])
+    _, _, gap, cond = O.emi(g["coh"])
+    tol = O.phase_tolerance(cond, gap, eps=EPS32)
+    assert np.all(np.abs(np.angle(ph * np.conj(g["ph"]))).max(-1) <= tol)
+    np.testing.assert_allclose(mb.ds_temp_coh(g["coh"], g["ph"]), g["t_coh"], atol=1e-6)
+    np.testing.assert_allclose(mb.temp_coh(g["coh"], g["ph"]), g["t_coh_pqm"], atol=1e-6)
+
+
+@pytest.mark.parametrize("name,size", [("c0", 64), ("c1", 40), ("c2", 40), ("c3", 20)])
+def test_emi_vs_fp64_oracle(cuda, name, size):
+    cfg = CONFIGS[name].scaled(nlines=size, width=size)
+    z = make_stack(cfg).numpy()
+    p = O.ks_test(O.intensity(z), cfg.az_half_win, cfg.r_half_win)
+    is_shp, num = O.select_shp(p, cfg.p_max)
+    idx, pc = O.ds_candidates(is_shp, num, 1)
+    coh = O.emperical_co_pc(z, idx, pc).astype(np.complex64)
+    ph_r, q_r, gap, cond = O.emi(coh)
+    ph, q = mb.emi(coh)
+    tol = O.phase_tolerance(cond, gap, eps=1e3 * EPS64, floor=1e-9)
+    err = np.abs(np.angle(ph * np.conj(ph_r))).max(-1)
+    assert np.all(err <= tol), (err / tol).max()
+    np.testing.assert_allclose(q, q_r.astype(np.float32), rtol=1e-5, atol=1e-5 * np.abs(q_r).max())
+    # well-conditioned points within 1 mrad
+    well = tol < 1e-6
+    assert err[well].max(initial=0) < 1e-3
+
+
+def test_emi_edges(cuda):
+    # N = 2 and N = 3 with exact coherence, reference image other than 0
+    for n in (2, 3, 5):
+        phi = np.linspace(0, 1, n)
+        g = 0.7 * np.exp(1j * (phi[:, None] - phi[None, :]))
+        np.fill_diagonal(g, 1)
+        r, s = np.triu_indices(n, 1)
+        coh = g[r, s][None].astype(np.complex64)
+        for ref in range(n):
+            ph, q = mb.emi(coh, ref=ref)
+            ph_r, q_r, _, _ = O.emi(coh, ref=ref)
+            np.testing.assert_allclose(ph, ph_r, atol=1e-6)
+            np.testing.assert_allclose(q, q_r, rtol=1e-6)
+    empty = mb.emi(np.zeros((0, 6), np.complex64))
+    assert empty[0].shape == (0, 4)
+    with pytest.raises(ValueError):
+        mb.emi(np.zeros((3, 7), np.complex64))
+
+
+def test_temp_coh_variants(cuda):
+    rng = np.random.default_rng(9)
+    n = 12
+    coh = (rng.standard_normal((300, 66)) + 1j * rng.standard_normal((300, 66))).astype(np.complex64)
+    ph = (rng.standard_normal((300, n)) + 1j * rng.standard_normal((300, n))).astype(np.complex64)
+    np.testing.assert_allclose(mb.temp_coh(coh, ph), O.temp_coh(coh, ph), atol=2e-6)
+    unit = ph / np.abs(ph)
+    np.testing.assert_allclose(mb.ds_temp_coh(coh, unit), O.ds_temp_coh(coh, unit), atol=2e-6)
+    pairs = mb.TempNet.from_bandwidth(n, 2).image_pairs
+    c2 = coh[:, :pairs.shape[0]]
+    np.testing.assert_allclose(mb.temp_coh(c2, ph, pairs), O.temp_coh(c2, ph, pairs), atol=2e-6)
+    ras = mb.temp_coh(coh.reshape(15, 20, 66), ph.reshape(15, 20, n))
+    assert ras.shape == (15, 20)
+    # inputs are not modified
+    c0 = coh.copy()
+    mb.temp_coh(coh, ph)
+    np.testing.assert_array_equal(coh, c0)
+
+
+def test_torch_in_torch_out(cuda, golden):
+    g = golden("co_small.npz")
+    c = torch.from_numpy(g["coh"]).to(cuda)
+    ph, q = mb.emi(c)
+    assert isinstance(ph, torch.Tensor) and ph.is_cuda and ph.dtype == torch.complex64
+    t = mb.ds_temp_coh(c, ph)
+    assert t.is_cuda and t.dtype == torch.float32
+
+
+# ----------------------------------------------------------------------------- chain
+def test_fused_helper_equals_separate_calls(cuda, golden):
+    g = golden("chain_small.npz")
+    idx = g["idx"]
+    pc = np.unpackbits(g["is_shp_bits"]).astype(bool).reshape(48, 48, 11, 11)[tuple(idx.T)]
+    ph_f, q_f, t_f = mb.emperical_co_emi_temp_coh_pc(g["rslc"], idx, pc, batch_size=100)
+    coh = mb.emperical_co_pc(g["rslc"], idx, pc)
+    ph, q = mb.emi(coh)
+    t = mb.ds_temp_coh(coh, ph)
+    np.testing.assert_array_equal(ph_f, ph)
+    np.testing.assert_array_equal(q_f, q)
+    np.testing.assert_array_equal(t_f, t)
+
+
+def test_device_chain_vs_reference_fixture(cuda, golden):
+    g = golden("chain_small.npz")
+    azh, rh = (int(v) for v in g["win"])
+    ch = DsChain(48, 48, 17, azh, rh, p_max=float(g["p_max"]), min_shp=int(g["min_shp"]), batch=100)
+    res = ch.run(torch.from_numpy(g["rslc"]).to(cuda))
+    np.testing.assert_array_equal(np.packbits(res.is_shp.cpu().numpy().astype(bool).reshape(-1)), g["is_shp_bits"])
+    np.testing.assert_array_equal(res.shp_num.cpu().numpy(), g["shp_num"])
+    np.testing.assert_array_equal(res.idx.cpu().numpy(), g["idx"])
+    coh = O.emperical_co_pc(g["rslc"], g["idx"], np.unpackbits(g["is_shp_bits"]).astype(bool).reshape(
+        48, 48, 11, 11)[tuple(g["idx"].T)])
+    _, _, gap, cond = O.emi(coh.astype(np.complex64))
+    tol = O.phase_tolerance(cond, gap, eps=EPS32)
+    err = np.abs(np.angle(res.ph.cpu().numpy() * np.conj(g["ph"]))).max(-1)
+    assert np.all(err <= tol), (err / tol).max()
+    well = tol < 1e-3
+    assert np.abs(res.t_coh.cpu().numpy() - g["t_coh"])[well].max(initial=0) < 1e-3
+
+
+@pytest.mark.parametrize("name,size", [("c0", 200), ("c1", 96), ("c2", 96)])
+def test_device_chain_vs_oracle(cuda, name, size):
+    cfg = CONFIGS[name].scaled(nlines=size, width=size)
+    z = make_stack(cfg)
+    ref = O.chain(z.numpy(), cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp)
+    res = DsChain(size, size, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp,
+                  batch=4096).run(z.to(cuda))
+    np.testing.assert_array_equal(res.is_shp.cpu().numpy().astype(bool), ref["is_shp"])
+    np.testing.assert_array_equal(res.shp_num.cpu().numpy(), ref["shp_num"])
+    np.testing.assert_array_equal(res.idx.cpu().numpy(), ref["idx"])
+    assert res.n_ds == len(ref["idx"])
+    if res.n_ds == 0:
+        return
+    # coherence in FP32 vs FP64: the phase error budget scales with cond / gap
+    tol = O.phase_tolerance(ref["cond"], ref["gap"], eps=EPS32)
+    err = np.abs(np.angle(res.ph.cpu().numpy() * np.conj(ref["ph"]))).max(-1)
+    assert np.all(err <= tol), (err / tol).max()
+    well = tol < 1e-3
+    assert np.abs(res.t_coh.cpu().numpy() - ref["t_coh"])[well].max(initial=0) < 1e-3
