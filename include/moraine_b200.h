@@ -48,10 +48,10 @@ enum {
 
 /* Arithmetic of the coherence Gram and of EMI. */
 enum {
-  MR_PREC_FP32 = 0,   /* FP32 SIMT Gram; EMI in FP64 */
+  MR_PREC_FP32 = 0,   /* FP32 SIMT Gram; FP32 EMI reduction */
   MR_PREC_BF16 = 1,   /* BF16 tensor-core Gram, FP32 accumulate */
   MR_PREC_BF16X3 = 2, /* BF16 hi/lo split tensor-core Gram (3 products) */
-  MR_PREC_FP64 = 3,   /* FP64 Gram */
+  MR_PREC_FP64 = 3,   /* FP64 Gram; FP64 EMI */
 };
 
 /* Limits of this build. */
@@ -132,14 +132,15 @@ int mr_uncompress_coh(const mr_complex64* coh, int64_t n, int nimages,
  * Replaces moraine.pl.emi (moraine/pl.py:68-77; GPU :19-42, CPU :46-65): for every
  * point, M = inv(|Gamma|) o Gamma from the full-triangle compressed coherence, its
  * algebraically smallest eigenpair (lambda, v), ph = v conj(v[ref]) / |v conj(v[ref])|,
- * emi_quality = lambda. inv(|Gamma|) by pivoted Gauss-Jordan, eigenpair by Householder
- * tridiagonalisation, Sturm bisection and inverse iteration, all in FP64.
+ * emi_quality = lambda. inv(|Gamma|) by pivoted Gauss-Jordan in FP64; eigenpair by
+ * Householder tridiagonalisation, Sturm bisection and inverse iteration in the arithmetic
+ * given by precision (MR_PREC_FP32 or MR_PREC_FP64; FP64 throughout when nimages > 128).
  * t_coh (may be NULL) receives moraine.pl.ds_temp_coh of the result (moraine/pl.py:126)
  * computed in the same pass. workspace: >= mr_emi_workspace_bytes(). */
 size_t mr_emi_workspace_bytes(int64_t n_pc, int nimages);
-int mr_emi(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, mr_complex64* ph,
-           float* emi_quality, float* t_coh, void* workspace, size_t workspace_bytes,
-           mr_stream_t stream);
+int mr_emi(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, int precision,
+           mr_complex64* ph, float* emi_quality, float* t_coh, void* workspace,
+           size_t workspace_bytes, mr_stream_t stream);
 
 /* ---------------------------------------------------------------- temporal coherence
  * Replaces moraine.pl.ds_temp_coh (moraine/pl.py:126-145; kernel :104-123):

@@ -37,7 +37,7 @@ _SIGNATURES = {
     "mr_emperical_co": (c_int, [P, c_int, c_int, c_int, P, c_int, c_int, P, P, P]),
     "mr_uncompress_coh": (c_int, [P, c_int64, c_int, P, c_int, P, P]),
     "mr_emi_workspace_bytes": (c_size_t, [c_int64, c_int]),
-    "mr_emi": (c_int, [P, c_int64, c_int, c_int, P, P, P, P, c_size_t, P]),
+    "mr_emi": (c_int, [P, c_int64, c_int, c_int, c_int, P, P, P, P, c_size_t, P]),
     "mr_ds_temp_coh": (c_int, [P, P, c_int64, c_int, P, c_int, P, P]),
     "mr_temp_coh": (c_int, [P, P, c_int64, c_int, P, c_int, P, P]),
 }

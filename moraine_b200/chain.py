@@ -43,6 +43,9 @@ class DsChain:
         self.win = self.az_win * self.r_win
         self.p_max, self.min_shp = float(p_max), int(min_shp)
         self.prec = _lib.PREC[precision]
+        # EMI reduction in FP64 only with an FP64 Gram; FP32 otherwise (its rounding is
+        # below the FP32/BF16 coherence error it starts from)
+        self.emi_prec = _lib.PREC["fp64"] if precision == "fp64" else _lib.PREC["fp32"]
         self.timing = timing
         self.npairs = nimages * (nimages - 1) // 2
         npix = nlines * width
@@ -95,8 +98,9 @@ class DsChain:
                       self.is_shp.data_ptr(), 1, self.az_win, self.r_win, None, self.npairs, self.coh.data_ptr(),
                       self.prec, s)
             mark("coherence")
-            _lib.call("mr_emi", self.coh.data_ptr(), nb, n, 0, self.ph[b0].data_ptr(), self.quality[b0:].data_ptr(),
-                      self.t_coh[b0:].data_ptr(), self.emi_ws.data_ptr(), self.emi_ws.numel(), s)
+            _lib.call("mr_emi", self.coh.data_ptr(), nb, n, 0, self.emi_prec, self.ph[b0].data_ptr(),
+                      self.quality[b0:].data_ptr(), self.t_coh[b0:].data_ptr(), self.emi_ws.data_ptr(),
+                      self.emi_ws.numel(), s)
             mark("emi_tcoh")
         stage = {}
         if self.timing:

@@ -244,6 +244,8 @@ extern "C" int mr_emperical_co_pc(const mr_complex64* rslc, int nlines, int widt
                                   const int32_t* idx, int64_t n_pc, const uint8_t* mask, int mask_stride,
                                   int az_win, int r_win, const int32_t* image_pairs, int n_pairs,
                                   mr_complex64* coh, int precision, mr_stream_t stream) {
+  MR_REQUIRE(n_pc >= 0, "emperical_co_pc: negative n_pc");
+  if (n_pc == 0) return MR_OK;
   MR_REQUIRE(rslc && idx && mask && coh, "emperical_co_pc: NULL pointer");
   MR_REQUIRE(nlines > 0 && width > 0 && nimages >= 2, "emperical_co_pc: bad stack shape");
   MR_REQUIRE(az_win > 0 && r_win > 0 && (az_win & 1) && (r_win & 1),

@@ -1,0 +1,572 @@
+// EMI for N <= 128, one CTA of 256 threads per point.
+//
+// Gauss-Jordan in registers (gj_tile): the padded 16NB x 16NB matrix |Gamma| is held by a
+//   16 x 16 thread grid, thread (tx, ty) owning rows ty + 16 ib and columns tx + 16 jb.
+//   Rows are never swapped: at step k the half-warp owning column k finds the pivot row
+//   p_k among the rows not yet used (largest |a|) and publishes column k through a
+//   double-buffered shared vector; every column group fetches row p_k by shuffles. One
+//   barrier per step. The result R satisfies inv[k][p_j] = R[p_k][j].
+// Householder reduction (tridiag_full): M = inv(|Gamma|) o Gamma in full Hermitian storage
+//   in shared memory (odd row pitch). Step k's rank-2 update is fused with the product of
+//   step k+1: a pair of threads owns each row of the trailing block, updates it and
+//   accumulates (M u)_i, so no cross-lane reduction is needed beyond the pair. Warp 0
+//   finishes step k-1 and forms reflector k in shared vectors between the two barriers of
+//   each step.
+// Kernels:
+//   fused_kernel<NB>        FP32: inverse in registers, M written straight to shared memory.
+//   inverse_kernel<NB>      FP64: inverse in registers, lower triangle written to the workspace,
+//   eig_kernel              then M formed from it in shared memory and reduced in FP64.
+// Both end with the common EMI tail (emi_common.cuh).
+#include <algorithm>
+
+#include "emi_common.cuh"
+
+namespace mr {
+namespace emi {
+namespace {
+
+constexpr int kMaxFastN = 128;
+
+template <typename T, int NB>
+struct GjShared {
+  T col[2][16 * NB];
+  int piv[2];
+  int piv_of_step[16 * NB];
+  int step_of_row[16 * NB];
+};
+
+// |Gamma| of point c into the register tile (identity on the padding).
+template <typename T, int NB>
+__device__ __forceinline__ void load_abs_gamma(T (&a)[NB][NB], unsigned& used, const float2* __restrict__ c, int n,
+                                               int tx, int ty) {
+  used = 0;
+#pragma unroll
+  for (int ib = 0; ib < NB; ++ib) {
+    const int i = ty + 16 * ib;
+    if (i >= n) used |= 1u << ib;  // padding rows never pivot
+#pragma unroll
+    for (int jb = 0; jb < NB; ++jb) {
+      const int j = tx + 16 * jb;
+      T v = (i == j) ? T(1) : T(0);
+      if (i < n && j < n && i != j) {
+        const float2 g = c[i < j ? triu_index(i, j, n) : triu_index(j, i, n)];
+        v = (T)sqrt((double)g.x * g.x + (double)g.y * g.y);
+      }
+      a[ib][jb] = v;
+    }
+  }
+}
+
+// a[ib][kb] for a CTA-uniform kb (a switch instead of per-element selects).
+template <typename T, int NB>
+__device__ __forceinline__ T col_of(const T (&a)[NB][NB], int ib, int kb) {
+  T v = 0;
+  switch (kb) {
+    case 0: v = a[ib][0]; break;
+    case 1: if (NB > 1) v = a[ib][1 < NB ? 1 : 0]; break;
+    case 2: if (NB > 2) v = a[ib][2 < NB ? 2 : 0]; break;
+    case 3: if (NB > 3) v = a[ib][3 < NB ? 3 : 0]; break;
+    case 4: if (NB > 4) v = a[ib][4 < NB ? 4 : 0]; break;
+    case 5: if (NB > 5) v = a[ib][5 < NB ? 5 : 0]; break;
+    case 6: if (NB > 6) v = a[ib][6 < NB ? 6 : 0]; break;
+    default: if (NB > 7) v = a[ib][7 < NB ? 7 : 0]; break;
+  }
+  return v;
+}
+
+template <typename T, int NB, int KB>
+__device__ __forceinline__ void set_col(T (&a)[NB][NB], int ib, T v) {
+  if (KB < NB) a[ib][KB < NB ? KB : 0] = v;
+}
+
+// In-place Gauss-Jordan inverse with partial pivoting on the register tile. Returns true
+// when a zero pivot was met (the matrix is singular).
+template <typename T, int NB>
+__device__ bool gj_tile(T (&a)[NB][NB], unsigned used, int n, int tx, int ty, GjShared<T, NB>& s) {
+  const int tid = threadIdx.x;
+  const unsigned half = (tx & 1) ? 0xFFFF0000u : 0x0000FFFFu;
+  bool singular = false;
+  for (int k = 0; k < n; ++k) {
+    const int buf = k & 1, kb = k >> 4;
+    const bool owner = tx == (k & 15);
+    if (owner) {  // the half-warp owning column k: publish it, find the pivot
+      T best = T(-1);
+      int bi = -1;
+#pragma unroll
+      for (int ib = 0; ib < NB; ++ib) {
+        const T v = col_of<T, NB>(a, ib, kb);
+        s.col[buf][ty + 16 * ib] = v;
+        const T av = fabs(v);
+        if (!(used & (1u << ib)) && av > best) { best = av; bi = ty + 16 * ib; }
+      }
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) {
+        const T ob = __shfl_xor_sync(half, best, o, 16);
+        const int oi = __shfl_xor_sync(half, bi, o, 16);
+        if (ob > best || (ob == best && oi >= 0 && (bi < 0 || oi < bi))) { best = ob; bi = oi; }
+      }
+      if (ty == 0) s.piv[buf] = bi;
+    }
+    __syncthreads();
+    const int p = s.piv[buf];
+    T pv = s.col[buf][p];
+    if (pv == T(0)) { singular = true; pv = T(1); }
+    const T rp = T(1) / pv;
+    if (ty == (p & 15)) used |= 1u << (p >> 4);
+    if (tid == 0) { s.piv_of_step[k] = p; s.step_of_row[p] = k; }
+    const int pl = p & 15;
+    // pivot row (scaled) from row lane pl of this column group; p >> 4 is CTA-uniform
+    T r[NB];
+    switch (p >> 4) {
+#define MR_GJ_ROW(PB)                                                                  \
+  case PB:                                                                             \
+    if (PB < NB) {                                                                     \
+      _Pragma("unroll") for (int jb = 0; jb < NB; ++jb) r[jb] =                        \
+          __shfl_sync(0xffffffffu, a[PB < NB ? PB : 0][jb], pl, 16) * rp;              \
+    }                                                                                  \
+    break;
+      MR_GJ_ROW(0) MR_GJ_ROW(1) MR_GJ_ROW(2) MR_GJ_ROW(3) MR_GJ_ROW(4) MR_GJ_ROW(5) MR_GJ_ROW(6)
+      default: MR_GJ_ROW(7)
+#undef MR_GJ_ROW
+    }
+    // a -= f_i r_j everywhere, with f_p = pv - 1 so that the pivot row becomes r
+#pragma unroll
+    for (int ib = 0; ib < NB; ++ib) {
+      const int i = ty + 16 * ib;
+      const T f = (i == p) ? pv - T(1) : s.col[buf][i];
+#pragma unroll
+      for (int jb = 0; jb < NB; ++jb) a[ib][jb] -= f * r[jb];
+    }
+    if (owner) {  // column k: delta_ip - f_i / pv
+#pragma unroll
+      for (int ib = 0; ib < NB; ++ib) {
+        const int i = ty + 16 * ib;
+        const T v = (i == p) ? rp : -s.col[buf][i] * rp;
+        switch (kb) {
+          case 0: set_col<T, NB, 0>(a, ib, v); break;
+          case 1: set_col<T, NB, 1>(a, ib, v); break;
+          case 2: set_col<T, NB, 2>(a, ib, v); break;
+          case 3: set_col<T, NB, 3>(a, ib, v); break;
+          case 4: set_col<T, NB, 4>(a, ib, v); break;
+          case 5: set_col<T, NB, 5>(a, ib, v); break;
+          case 6: set_col<T, NB, 6>(a, ib, v); break;
+          default: set_col<T, NB, 7>(a, ib, v); break;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  return singular;
+}
+
+// ----------------------------------------------------------------- full-storage reduction
+template <typename T>
+struct TriShared {
+  using C = typename C2<T>::type;
+  C* M;       // n x pitch
+  int pitch;  // odd
+  C* pv;      // [2][n] products of the last two steps
+  C* vec;     // [3][n]: u_k and u_{k-1} (by step parity), w_{k-1}
+  C* e;
+  C* z;
+  double2* phs;
+  T* d;
+  T* tau;
+  T* b;
+  T* b2;
+  T* y;
+  T* w1;
+  T* w2;
+  T* w3;
+  Red* red;
+};
+
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+__host__ __device__ inline int odd_pitch(int n) { return n | 1; }
+
+template <typename T>
+__host__ __device__ inline size_t tri_bytes(int n) {
+  using C = typename C2<T>::type;
+  size_t o = align16((size_t)n * odd_pitch(n) * sizeof(C));
+  o = align16(o + 2 * (size_t)n * sizeof(C));
+  o = align16(o + 3 * (size_t)n * sizeof(C));
+  o = align16(o + 2 * (size_t)n * sizeof(C));
+  o = align16(o + (size_t)n * sizeof(double2));
+  o = align16(o + 8 * (size_t)n * sizeof(T));
+  return o + sizeof(Red);
+}
+
+template <typename T>
+__device__ inline TriShared<T> tri_layout(unsigned char* base, int n) {
+  using C = typename C2<T>::type;
+  TriShared<T> s;
+  s.pitch = odd_pitch(n);
+  size_t o = 0;
+  s.M = reinterpret_cast<C*>(base + o);
+  o = align16(o + (size_t)n * s.pitch * sizeof(C));
+  s.pv = reinterpret_cast<C*>(base + o);
+  o = align16(o + 2 * (size_t)n * sizeof(C));
+  s.vec = reinterpret_cast<C*>(base + o);
+  o = align16(o + 3 * (size_t)n * sizeof(C));
+  s.e = reinterpret_cast<C*>(base + o);
+  s.z = s.e + n;
+  o = align16(o + 2 * (size_t)n * sizeof(C));
+  s.phs = reinterpret_cast<double2*>(base + o);
+  o = align16(o + (size_t)n * sizeof(double2));
+  s.d = reinterpret_cast<T*>(base + o);
+  s.tau = s.d + n;
+  s.b = s.tau + n;
+  s.b2 = s.b + n;
+  s.y = s.b2 + n;
+  s.w1 = s.y + n;
+  s.w2 = s.w1 + n;
+  s.w3 = s.w2 + n;
+  o = align16(o + 8 * (size_t)n * sizeof(T));
+  s.red = reinterpret_cast<Red*>(base + o);
+  return s;
+}
+
+// a -= ui conj(wj) + wi conj(uj)
+template <typename C> __device__ __forceinline__ void rank2(C& a, C ui, C wj, C wi, C uj) {
+  a.x -= ui.x * wj.x + ui.y * wj.y + wi.x * uj.x + wi.y * uj.y;
+  a.y -= ui.y * wj.x - ui.x * wj.y + wi.y * uj.x - wi.x * uj.y;
+}
+
+// Householder reduction of the Hermitian M (full storage in s.M) to tridiagonal (s.d, s.e),
+// reflector k stored in column k (rows k+1..n-1) with scalar s.tau[k]. Whole CTA.
+template <typename T>
+__device__ void tridiag_full(const TriShared<T>& s, int n) {
+  using C = typename C2<T>::type;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int P = s.pitch;
+  C* M = s.M;
+  C* wp = s.vec + 2 * n;  // w_{k-1}
+  const int rr = tid >> 1, h = tid & 1;  // row slot and half of the pair
+  for (int k = 0; k + 2 < n; ++k) {
+    C* up = s.vec + ((k + 1) & 1) * n;  // u_{k-1}
+    C* uc = s.vec + (k & 1) * n;        // u_k
+    // ---- warp 0: w_{k-1} = p - K u_{k-1}; column k up to date; reflector k
+    if (wid == 0) {
+      const T tau_prev = k > 0 ? s.tau[k - 1] : T(0);
+      const bool pending = tau_prev != T(0);
+      if (pending) {
+        const C* p = s.pv + ((k + 1) & 1) * n;
+        T dot = 0;
+        for (int i = k + lane; i < n; i += 32) {
+          const C pi = p[i], ui = up[i];
+          wp[i] = pi;
+          dot += ui.x * pi.x + ui.y * pi.y;
+        }
+        const T K = T(0.5) * tau_prev * warp_sum(dot);
+        for (int i = k + lane; i < n; i += 32) { wp[i].x -= K * up[i].x; wp[i].y -= K * up[i].y; }
+        __syncwarp();
+      }
+      C ukk = mk<T>(0, 0), wkk = mk<T>(0, 0);
+      if (pending) { ukk = up[k]; wkk = wp[k]; }
+      T xn2 = 0;
+      for (int i = k + lane; i < n; i += 32) {
+        C x = M[(size_t)i * P + k];
+        if (pending) {
+          rank2(x, up[i], wkk, wp[i], ukk);
+          M[(size_t)i * P + k - 1] = up[i];  // reflector k-1 (rows >= k) into column k-1
+        }
+        uc[i] = x;
+        if (i >= k + 2) xn2 += x.x * x.x + x.y * x.y;
+      }
+      xn2 = warp_sum(xn2);
+      __syncwarp();
+      const C alpha = uc[k + 1];
+      T tau_k = 0;
+      C ek = alpha;
+      if (xn2 != T(0)) {
+        const T aa = sqrt(alpha.x * alpha.x + alpha.y * alpha.y);
+        const T nrm = sqrt(aa * aa + xn2);
+        const C ph1 = aa > T(0) ? mk<T>(alpha.x / aa, alpha.y / aa) : mk<T>(1, 0);
+        tau_k = T(2) / ((aa + nrm) * (aa + nrm) + xn2);
+        ek = mk<T>(-ph1.x * nrm, -ph1.y * nrm);
+        if (lane == 0) uc[k + 1] = mk<T>(ph1.x * (aa + nrm), ph1.y * (aa + nrm));
+      }
+      if (lane == 0) { s.d[k] = uc[k].x; s.e[k] = ek; s.tau[k] = tau_k; }
+    }
+    __syncthreads();
+    // ---- row pairs: step k-1's update on rows/cols >= k+1 and p_k = tau_k M u_k
+    const bool pending = k > 0 && s.tau[k - 1] != T(0);
+    const T tau_k = s.tau[k];
+    const int i = k + 1 + rr;
+    if ((pending || tau_k != T(0)) && i < n) {
+      C* row = M + (size_t)i * P;
+      C upi = mk<T>(0, 0), wpi = mk<T>(0, 0);
+      if (pending) { upi = up[i]; wpi = wp[i]; }
+      C acc0 = mk<T>(0, 0), acc1 = mk<T>(0, 0);
+      int j = k + 1 + h;
+      for (; j + 2 < n; j += 4) {
+        C a0 = row[j], a1 = row[j + 2];
+        if (pending) {
+          rank2(a0, upi, wp[j], wpi, up[j]);
+          rank2(a1, upi, wp[j + 2], wpi, up[j + 2]);
+          row[j] = a0;
+          row[j + 2] = a1;
+        }
+        const C u0 = uc[j], u1 = uc[j + 2];
+        acc0.x += a0.x * u0.x - a0.y * u0.y;
+        acc0.y += a0.x * u0.y + a0.y * u0.x;
+        acc1.x += a1.x * u1.x - a1.y * u1.y;
+        acc1.y += a1.x * u1.y + a1.y * u1.x;
+      }
+      if (j < n) {
+        C a0 = row[j];
+        if (pending) { rank2(a0, upi, wp[j], wpi, up[j]); row[j] = a0; }
+        const C u0 = uc[j];
+        acc0.x += a0.x * u0.x - a0.y * u0.y;
+        acc0.y += a0.x * u0.y + a0.y * u0.x;
+      }
+      acc0 = cadd(acc0, acc1);
+      // the pair (lanes 2r, 2r+1) is active together: i depends only on tid >> 1
+      const unsigned pair = 3u << (lane & ~1);
+      acc0.x += __shfl_xor_sync(pair, acc0.x, 1);
+      acc0.y += __shfl_xor_sync(pair, acc0.y, 1);
+      if (h == 0 && tau_k != T(0)) s.pv[(k & 1) * n + i] = mk<T>(tau_k * acc0.x, tau_k * acc0.y);
+    }
+    __syncthreads();
+  }
+  // last pending update (step n-3) on the trailing 2 x 2 block; reflector n-3 stored
+  if (wid == 0) {
+    if (n >= 3 && s.tau[n - 3] != T(0)) {
+      const T tau_prev = s.tau[n - 3];
+      const C* up = s.vec + ((n - 3) & 1) * n;
+      const C* p = s.pv + ((n - 3) & 1) * n;
+      T dot = 0;
+      for (int i = n - 2 + lane; i < n; i += 32) {
+        const C pi = p[i], ui = up[i];
+        wp[i] = pi;
+        dot += ui.x * pi.x + ui.y * pi.y;
+      }
+      const T K = T(0.5) * tau_prev * warp_sum(dot);
+      for (int i = n - 2 + lane; i < n; i += 32) { wp[i].x -= K * up[i].x; wp[i].y -= K * up[i].y; }
+      __syncwarp();
+      if (lane < 3) {
+        const int i = (lane == 0) ? n - 2 : n - 1, j = (lane == 2) ? n - 1 : n - 2;
+        rank2(M[(size_t)i * P + j], up[i], wp[j], wp[i], up[j]);
+      }
+      for (int i = n - 2 + lane; i < n; i += 32) M[(size_t)i * P + n - 3] = up[i];
+      __syncwarp();
+    }
+    if (lane == 0) {
+      s.d[n - 2] = M[(size_t)(n - 2) * P + n - 2].x;
+      s.d[n - 1] = M[(size_t)(n - 1) * P + n - 1].x;
+      s.e[n - 2] = M[(size_t)(n - 1) * P + n - 2];
+    }
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ __forceinline__ void finish(const TriShared<T>& s, int n, int ref, bool singular, float2* ph,
+                                       float* quality, float* tcoh, const float2* c, int64_t npairs) {
+  TailVecs<T> tv{s.d, s.e, s.tau, s.b, s.b2, s.y, s.w1, s.w2, s.w3, s.z, s.phs};
+  const int P = s.pitch;
+  typename C2<T>::type* M = s.M;
+  auto uk = [&](int k, int i) { return M[(size_t)(k + 1 + i) * P + k]; };
+  tail<T>(n, ref, tv, uk, *s.red, singular, ph, quality, tcoh, c, npairs);
+}
+
+// ----------------------------------------------------------------- FP32: one kernel
+template <int NB>
+__global__ void __launch_bounds__(kThreads, 2) fused_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
+                                                            int ref, float2* __restrict__ ph,
+                                                            float* __restrict__ quality, float* __restrict__ tcoh) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ GjShared<float, NB> gs;
+  const TriShared<float> s = tri_layout<float>(smem_raw, n);
+  const int tid = threadIdx.x, tx = tid >> 4, ty = tid & 15;
+  const int64_t npairs = (int64_t)n * (n - 1) / 2;
+  const int P = s.pitch;
+  for (int64_t pt = blockIdx.x; pt < n_pc; pt += gridDim.x) {
+    const float2* c = coh + pt * npairs;
+    float a[NB][NB];
+    unsigned used;
+    load_abs_gamma<float, NB>(a, used, c, n, tx, ty);
+    const bool singular = gj_tile<float, NB>(a, used, n, tx, ty, gs);
+    // M[kr][pc] = inv(|Gamma|)[kr][pc] * Gamma[kr][pc]
+#pragma unroll
+    for (int ib = 0; ib < NB; ++ib) {
+      const int r0 = ty + 16 * ib;
+      if (r0 >= n) continue;
+      const int kr = gs.step_of_row[r0];
+#pragma unroll
+      for (int jb = 0; jb < NB; ++jb) {
+        const int c0 = tx + 16 * jb;
+        if (c0 >= n) continue;
+        const int pc = gs.piv_of_step[c0];
+        float gx = 1.f, gy = 0.f;
+        if (kr != pc) {
+          const float2 g = c[kr < pc ? triu_index(kr, pc, n) : triu_index(pc, kr, n)];
+          gx = g.x;
+          gy = kr < pc ? g.y : -g.y;
+        }
+        s.M[(size_t)kr * P + pc] = make_float2(a[ib][jb] * gx, a[ib][jb] * gy);
+      }
+    }
+    __syncthreads();
+    tridiag_full<float>(s, n);
+    finish<float>(s, n, ref, singular, ph + pt * n, quality + pt, tcoh ? tcoh + pt : nullptr, c, npairs);
+  }
+}
+
+// ----------------------------------------------------------------- FP64: two kernels
+template <int NB>
+__global__ void __launch_bounds__(kThreads, 1) inverse_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
+                                                             double* __restrict__ ainv, uint8_t* __restrict__ sing) {
+  __shared__ GjShared<double, NB> gs;
+  const int tid = threadIdx.x, tx = tid >> 4, ty = tid & 15;
+  const int64_t npairs = (int64_t)n * (n - 1) / 2;
+  const int64_t npk = (int64_t)n * (n + 1) / 2;
+  for (int64_t pt = blockIdx.x; pt < n_pc; pt += gridDim.x) {
+    double a[NB][NB];
+    unsigned used;
+    load_abs_gamma<double, NB>(a, used, coh + pt * npairs, n, tx, ty);
+    const bool singular = gj_tile<double, NB>(a, used, n, tx, ty, gs);
+    double* out = ainv + pt * npk;
+#pragma unroll
+    for (int ib = 0; ib < NB; ++ib) {
+      const int r0 = ty + 16 * ib;
+      if (r0 >= n) continue;
+      const int kr = gs.step_of_row[r0];
+#pragma unroll
+      for (int jb = 0; jb < NB; ++jb) {
+        const int c0 = tx + 16 * jb;
+        if (c0 >= n) continue;
+        const int pc = gs.piv_of_step[c0];
+        if (kr >= pc) out[(int64_t)kr * (kr + 1) / 2 + pc] = a[ib][jb];
+      }
+    }
+    if (tid == 0) sing[pt] = singular ? 1 : 0;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) eig_kernel(const float2* __restrict__ coh, int64_t n_pc, int n, int ref,
+                                                       const double* __restrict__ ainv,
+                                                       const uint8_t* __restrict__ sing, float2* __restrict__ ph,
+                                                       float* __restrict__ quality, float* __restrict__ tcoh) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const TriShared<double> s = tri_layout<double>(smem_raw, n);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int64_t npairs = (int64_t)n * (n - 1) / 2;
+  const int64_t npk = (int64_t)n * (n + 1) / 2;
+  const int P = s.pitch;
+  for (int64_t pt = blockIdx.x; pt < n_pc; pt += gridDim.x) {
+    const float2* c = coh + pt * npairs;
+    const double* ai = ainv + pt * npk;
+    for (int e = tid; e < n * n; e += nt) {
+      const int i = e / n, j = e - i * n;
+      const int hi = max(i, j), lo = min(i, j);
+      double gx = 1.0, gy = 0.0;
+      if (i != j) {
+        const float2 g = c[triu_index(lo, hi, n)];
+        gx = g.x;
+        gy = i < j ? g.y : -g.y;
+      }
+      const double sc = ai[(int64_t)hi * (hi + 1) / 2 + lo];
+      s.M[(size_t)i * P + j] = make_double2(sc * gx, sc * gy);
+    }
+    __syncthreads();
+    tridiag_full<double>(s, n);
+    finish<double>(s, n, ref, sing[pt] != 0, ph + pt * n, quality + pt, tcoh ? tcoh + pt : nullptr, c, npairs);
+  }
+}
+
+int sub_batch(int n) {
+  const size_t np = (size_t)n * (n + 1) / 2;
+  const size_t per = np * sizeof(double) + 1;
+  return (int)std::max<size_t>(1024, std::min<size_t>(65536, (size_t)(1ull << 30) / per));
+}
+
+template <class K>
+int occupancy(K kernel, size_t smem) {
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kThreads, smem) != cudaSuccess) return 0;
+  return occ;
+}
+
+template <int NB>
+int launch_fused(const float2* coh, int64_t n_pc, int n, int ref, float2* ph, float* q, float* t, cudaStream_t s) {
+  const size_t smem = tri_bytes<float>(n);
+  MR_CUDA_TRY(cudaFuncSetAttribute(fused_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int occ = occupancy(fused_kernel<NB>, smem);
+  if (occ < 1) return fail(MR_ERR_UNSUPPORTED, "emi: %zu bytes of shared memory per CTA do not fit", smem);
+  const int64_t grid = std::min<int64_t>(n_pc, (int64_t)sm_count() * occ);
+  fused_kernel<NB><<<(unsigned)grid, kThreads, smem, s>>>(coh, n_pc, n, ref, ph, q, t);
+  return check_launch("emi (fp32)");
+}
+
+template <int NB>
+int launch_inverse(const float2* coh, int64_t n, int nimg, double* ainv, uint8_t* sing, cudaStream_t s) {
+  const int occ = std::max(1, occupancy(inverse_kernel<NB>, 0));
+  const int64_t grid = std::min<int64_t>(n, (int64_t)sm_count() * occ);
+  inverse_kernel<NB><<<(unsigned)grid, kThreads, 0, s>>>(coh, n, nimg, ainv, sing);
+  return check_launch("emi inverse (fp64)");
+}
+
+int launch_eig64(const float2* c, int64_t nb, int n, int ref, const double* ainv, const uint8_t* sing, float2* ph,
+                 float* quality, float* tcoh, cudaStream_t s) {
+  const size_t smem = tri_bytes<double>(n);
+  MR_CUDA_TRY(cudaFuncSetAttribute(eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int occ = occupancy(eig_kernel, smem);
+  if (occ < 1) return fail(MR_ERR_UNSUPPORTED, "emi: %zu bytes of shared memory per CTA do not fit", smem);
+  const int64_t grid = std::min<int64_t>(nb, (int64_t)sm_count() * occ);
+  eig_kernel<<<(unsigned)grid, kThreads, smem, s>>>(c, nb, n, ref, ainv, sing, ph, quality, tcoh);
+  return check_launch("emi eig (fp64)");
+}
+
+}  // namespace
+
+int fast_supported(int n) { return n >= 2 && n <= kMaxFastN; }
+
+size_t fast_workspace_bytes(int64_t n_pc, int n) {
+  const int64_t sub = std::min<int64_t>(n_pc, sub_batch(n));
+  const size_t np = (size_t)n * (n + 1) / 2;
+  return ((size_t)sub * np * sizeof(double) + 255) / 256 * 256 + (size_t)sub;
+}
+
+int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, float2* ph, float* quality,
+             float* tcoh, void* workspace, size_t workspace_bytes, cudaStream_t s) {
+  (void)workspace_bytes;
+  if (precision != MR_PREC_FP64) {
+    switch ((n + 15) / 16) {
+      case 1: case 2: return launch_fused<2>(coh, n_pc, n, ref, ph, quality, tcoh, s);
+      case 3: return launch_fused<3>(coh, n_pc, n, ref, ph, quality, tcoh, s);
+      case 4: return launch_fused<4>(coh, n_pc, n, ref, ph, quality, tcoh, s);
+      case 5: return launch_fused<5>(coh, n_pc, n, ref, ph, quality, tcoh, s);
+      case 6: return launch_fused<6>(coh, n_pc, n, ref, ph, quality, tcoh, s);
+      case 7: return launch_fused<7>(coh, n_pc, n, ref, ph, quality, tcoh, s);
+      default: return launch_fused<8>(coh, n_pc, n, ref, ph, quality, tcoh, s);
+    }
+  }
+  const int64_t sub = std::min<int64_t>(n_pc, sub_batch(n));
+  const size_t np = (size_t)n * (n + 1) / 2;
+  double* ainv = static_cast<double*>(workspace);
+  uint8_t* sing = static_cast<uint8_t*>(workspace) + ((size_t)sub * np * sizeof(double) + 255) / 256 * 256;
+  const int64_t npairs = (int64_t)n * (n - 1) / 2;
+  for (int64_t b0 = 0; b0 < n_pc; b0 += sub) {
+    const int64_t nb = std::min<int64_t>(sub, n_pc - b0);
+    const float2* c = coh + b0 * npairs;
+    int rc;
+    switch ((n + 15) / 16) {
+      case 1: case 2: rc = launch_inverse<2>(c, nb, n, ainv, sing, s); break;
+      case 3: rc = launch_inverse<3>(c, nb, n, ainv, sing, s); break;
+      case 4: rc = launch_inverse<4>(c, nb, n, ainv, sing, s); break;
+      case 5: rc = launch_inverse<5>(c, nb, n, ainv, sing, s); break;
+      case 6: rc = launch_inverse<6>(c, nb, n, ainv, sing, s); break;
+      case 7: rc = launch_inverse<7>(c, nb, n, ainv, sing, s); break;
+      default: rc = launch_inverse<8>(c, nb, n, ainv, sing, s); break;
+    }
+    if (rc) return rc;
+    rc = launch_eig64(c, nb, n, ref, ainv, sing, ph + b0 * n, quality + b0, tcoh ? tcoh + b0 : nullptr, s);
+    if (rc) return rc;
+  }
+  return MR_OK;
+}
+
+}  // namespace emi
+}  // namespace mr

@@ -96,11 +96,11 @@ using namespace mr;
 
 static int temp_coh_common(bool pqm, const mr_complex64* intf, const mr_complex64* ph, int64_t n, int nimages,
                            const int32_t* image_pairs, int n_pairs, float* t_coh, mr_stream_t stream) {
-  MR_REQUIRE(intf && ph && t_coh, "temp_coh: NULL pointer");
   MR_REQUIRE(nimages >= 2 && n >= 0, "temp_coh: bad shape");
   if (!image_pairs) n_pairs = nimages * (nimages - 1) / 2;
   MR_REQUIRE(n_pairs > 0, "temp_coh: no pairs");
   if (n == 0) return MR_OK;
+  MR_REQUIRE(intf && ph && t_coh, "temp_coh: NULL pointer");
   auto* c = reinterpret_cast<const float2*>(intf);
   auto* p = reinterpret_cast<const float2*>(ph);
   if (pqm)
@@ -122,10 +122,10 @@ extern "C" int mr_temp_coh(const mr_complex64* intf, const mr_complex64* rslc, i
 
 extern "C" int mr_uncompress_coh(const mr_complex64* coh, int64_t n, int nimages, const int32_t* image_pairs,
                                  int n_pairs, mr_complex64* out, mr_stream_t stream) {
-  MR_REQUIRE(coh && out, "uncompress_coh: NULL pointer");
   MR_REQUIRE(nimages >= 1 && n >= 0, "uncompress_coh: bad shape");
   if (!image_pairs) n_pairs = nimages * (nimages - 1) / 2;
   if (n == 0) return MR_OK;
+  MR_REQUIRE(coh && out, "uncompress_coh: NULL pointer");
   cudaStream_t s = as_stream(stream);
   auto* o = reinterpret_cast<float2*>(out);
   uncompress_fill_kernel<<<grid_for(n * nimages * nimages, 256), 256, 0, s>>>(o, n, nimages);

@@ -13,7 +13,7 @@ from .tnet import TempNet, nimage_from_npair
 __all__ = ["emi", "ds_temp_coh", "emperical_co_emi_temp_coh_pc"]
 
 
-def _emi_device(c: torch.Tensor, nimages: int, ref: int, want_tcoh: bool = False):
+def _emi_device(c: torch.Tensor, nimages: int, ref: int, want_tcoh: bool = False, precision: str = "fp64"):
     dev = c.device
     n_pc = c.shape[0]
     ph = torch.empty((n_pc, nimages), dtype=torch.complex64, device=dev)
@@ -21,24 +21,26 @@ def _emi_device(c: torch.Tensor, nimages: int, ref: int, want_tcoh: bool = False
     t = torch.empty((n_pc,), dtype=torch.float32, device=dev) if want_tcoh else None
     lib = _lib.load()
     ws = _dev.workspace(lib.mr_emi_workspace_bytes(n_pc, nimages), dev)
-    _lib.call("mr_emi", c.data_ptr(), n_pc, nimages, ref, ph.data_ptr(), q.data_ptr(), _dev.ptr(t), ws.data_ptr(),
-              ws.numel(), _dev.stream())
+    _lib.call("mr_emi", c.data_ptr(), n_pc, nimages, ref, _lib.PREC[precision], ph.data_ptr(), q.data_ptr(),
+              _dev.ptr(t), ws.data_ptr(), ws.numel(), _dev.stream())
     return ph, q, t
 
 
-def emi(coh, ref: int = 0):
+def emi(coh, ref: int = 0, precision: str = "fp64"):
     """EMI phase linking of compressed coherence ``(n_pc, n_pairs)`` (all pairs).
 
     Returns ``ph`` (n_pc, N) complex64 (unit modulus, ``ph[:, ref]`` real positive) and
     ``emi_quality`` (n_pc,) float32, the smallest eigenvalue of ``inv(|Gamma|) o Gamma``
-    (moraine/pl.py:19-77), computed in FP64.
+    (moraine/pl.py:19-77). ``precision`` (an addition to the reference signature):
+    ``"fp64"`` (default) or ``"fp32"`` for the eigen-reduction; the inverse of
+    ``|Gamma|`` is always FP64.
     """
     kind = _dev.kind_of(coh)
     dev = _dev.require_cuda()
     c = _dev.to_device(coh, torch.complex64, dev)
     nimages = nimage_from_npair(c.shape[-1])
     c2 = c.reshape(-1, c.shape[-1])
-    ph, q, _ = _emi_device(c2, nimages, int(ref))
+    ph, q, _ = _emi_device(c2, nimages, int(ref), precision=precision)
     ph = ph.reshape(tuple(c.shape[:-1]) + (nimages,))
     q = q.reshape(tuple(c.shape[:-1]))
     return _dev.from_device(ph, kind), _dev.from_device(q, kind)

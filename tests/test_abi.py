@@ -39,8 +39,9 @@ def test_version_and_sizes():
      _lib.MR_ERR_UNSUPPORTED),
     (lambda L: L.mr_ks_test(16, 10, 10, 17, 1, 1, 16, None, 0.05, None, None, 16, 10, None), _lib.MR_ERR_WORKSPACE),
     (lambda L: L.mr_ks_test(16, 10, 10, 17, 1, 1, 16, None, 0.05, 16, None, 16, 10**9, None), _lib.MR_ERR_INVALID),
-    (lambda L: L.mr_emi(16, 10, 17, 17, 16, 16, None, 16, 10**9, None), _lib.MR_ERR_INVALID),
-    (lambda L: L.mr_emi(16, 10, 1, 0, 16, 16, None, 16, 10**9, None), _lib.MR_ERR_INVALID),
+    (lambda L: L.mr_emi(16, 10, 17, 17, 0, 16, 16, None, 16, 10**9, None), _lib.MR_ERR_INVALID),
+    (lambda L: L.mr_emi(16, 10, 1, 0, 0, 16, 16, None, 16, 10**9, None), _lib.MR_ERR_INVALID),
+    (lambda L: L.mr_emi(16, 10, 17, 0, 1, 16, 16, None, 16, 10**9, None), _lib.MR_ERR_INVALID),
     (lambda L: L.mr_emperical_co_pc(16, 10, 10, 17, 16, 5, 16, 0, 4, 3, None, 0, 16, 0, None), _lib.MR_ERR_INVALID),
     (lambda L: L.mr_emperical_co_pc(16, 10, 10, 17, 16, 5, 16, 2, 3, 3, None, 0, 16, 0, None), _lib.MR_ERR_INVALID),
     (lambda L: L.mr_ds_extract(16, None, 10, 10, 9, 3, 16, 16, 100, 16, 16, 10**6, None), _lib.MR_ERR_INVALID),

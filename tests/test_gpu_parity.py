@@ -11,6 +11,8 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 EPS32, EPS64 = 6e-8, 1.2e-16
+# relative error of a coherence accumulated in FP32 over up to ~500 looks (sqrt(S) eps32)
+EPS_GRAM32 = 2e-6
 
 
 # ----------------------------------------------------------------------------- KS
@@ -117,8 +119,10 @@ def test_emi_vs_reference_fixture(cuda, golden):
     np.testing.assert_allclose(mb.temp_coh(g["coh"], g["ph"]), g["t_coh_pqm"], atol=1e-6)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("name,size", [("c0", 64), ("c1", 40), ("c2", 40), ("c3", 20)])
-def test_emi_vs_fp64_oracle(cuda, name, size):
+def test_emi_vs_fp64_oracle(cuda, name, size, precision):
+    """EMI alone on identical complex64 coherence: FP64 and FP32 reductions vs LAPACK FP64."""
     cfg = CONFIGS[name].scaled(nlines=size, width=size)
     z = make_stack(cfg).numpy()
     p = O.ks_test(O.intensity(z), cfg.az_half_win, cfg.r_half_win)
@@ -126,13 +130,22 @@ def test_emi_vs_fp64_oracle(cuda, name, size):
     idx, pc = O.ds_candidates(is_shp, num, 1)
     coh = O.emperical_co_pc(z, idx, pc).astype(np.complex64)
     ph_r, q_r, gap, cond = O.emi(coh)
-    ph, q = mb.emi(coh)
-    tol = O.phase_tolerance(cond, gap, eps=1e3 * EPS64, floor=1e-9)
+    ph, q = mb.emi(coh, precision=precision)
+    # complex64 output rounding bounds the floor; the arithmetic bounds the rest
+    eps = 1e3 * EPS64 if precision == "fp64" else 4 * EPS32
+    tol = O.phase_tolerance(cond, gap, eps=eps, floor=3e-7 if precision == "fp64" else 2e-6)
     err = np.abs(np.angle(ph * np.conj(ph_r))).max(-1)
-    assert np.all(err <= tol), (err / tol).max()
-    np.testing.assert_allclose(q, q_r.astype(np.float32), rtol=1e-5, atol=1e-5 * np.abs(q_r).max())
+    # |Gamma| numerically singular at this precision (e.g. a single look: |Gamma| = ones):
+    # the kernel reports NaN there; the reference's inv() raises for exactly singular input
+    singular = cond * (EPS32 if precision == "fp32" else EPS64) > 0.05
+    nan = np.isnan(err)
+    assert not np.any(nan & ~singular)
+    ok = ~nan
+    assert np.all(err[ok] <= tol[ok]), (err[ok] / tol[ok]).max()
+    qtol = (1e-5 if precision == "fp64" else 1e-5 * cond) * np.maximum(1, np.abs(q_r))
+    assert np.all(np.abs(q - q_r)[ok] <= qtol[ok])
     # well-conditioned points within 1 mrad
-    well = tol < 1e-6
+    well = cond / np.maximum(gap, 1e-12) < 1e3
     assert err[well].max(initial=0) < 1e-3
 
 
@@ -208,7 +221,7 @@ def test_device_chain_vs_reference_fixture(cuda, golden):
     coh = O.emperical_co_pc(g["rslc"], g["idx"], np.unpackbits(g["is_shp_bits"]).astype(bool).reshape(
         48, 48, 11, 11)[tuple(g["idx"].T)])
     _, _, gap, cond = O.emi(coh.astype(np.complex64))
-    tol = O.phase_tolerance(cond, gap, eps=EPS32)
+    tol = O.phase_tolerance(cond, gap, eps=EPS_GRAM32)
     err = np.abs(np.angle(res.ph.cpu().numpy() * np.conj(g["ph"]))).max(-1)
     assert np.all(err <= tol), (err / tol).max()
     well = tol < 1e-3
@@ -229,7 +242,7 @@ def test_device_chain_vs_oracle(cuda, name, size):
     if res.n_ds == 0:
         return
     # coherence in FP32 vs FP64: the phase error budget scales with cond / gap
-    tol = O.phase_tolerance(ref["cond"], ref["gap"], eps=EPS32)
+    tol = O.phase_tolerance(ref["cond"], ref["gap"], eps=EPS_GRAM32)
     err = np.abs(np.angle(res.ph.cpu().numpy() * np.conj(ref["ph"]))).max(-1)
     assert np.all(err <= tol), (err / tol).max()
     well = tol < 1e-3
