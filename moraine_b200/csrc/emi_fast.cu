@@ -12,11 +12,16 @@
 //   accumulates (M u)_i, so no cross-lane reduction is needed beyond the pair. Warp 0
 //   finishes step k-1 and forms reflector k in shared vectors between the two barriers of
 //   each step.
-// Kernels:
-//   fused_kernel<NB>        FP32: inverse in registers, M written straight to shared memory.
-//   inverse_kernel<NB>      FP64: inverse in registers, lower triangle written to the workspace,
-//   eig_kernel              then M formed from it in shared memory and reduced in FP64.
-// Both end with the common EMI tail (emi_common.cuh).
+// Three kernels per sub-batch of points, in FP32 or FP64 (template T):
+//   inverse_kernel<T, NB>  inv(|Gamma|) in registers -> workspace (lower triangle, packed);
+//   reduce_kernel<T>       M in shared memory, Householder reduction -> workspace (d, e, tau,
+//                          reflectors);
+//   tail_kernel<T>         one warp per point: smallest eigenvalue by Sturm multisection,
+//                          inverse iteration on the real tridiagonal, back-transformation,
+//                          normalisation to the reference image, temporal coherence.
+// Splitting by resource lets each stage run at its own occupancy: the serial, O(N)
+// tail of many points overlaps on one SM, and the register-bound inverse is not held
+// back by the shared memory of the reduction.
 #include <algorithm>
 
 #include "emi_common.cuh"
@@ -360,73 +365,58 @@ __device__ void tridiag_full(const TriShared<T>& s, int n) {
   __syncthreads();
 }
 
+// ----------------------------------------------------------------- workspace layout
+// Per point: inv(|Gamma|) lower triangle packed (np T), reflectors (column k rows
+// k+1..n-1, packed by column, nq complex T), d and tau (n T each), e (n complex T).
 template <typename T>
-__device__ __forceinline__ void finish(const TriShared<T>& s, int n, int ref, bool singular, float2* ph,
-                                       float* quality, float* tcoh, const float2* c, int64_t npairs) {
-  TailVecs<T> tv{s.d, s.e, s.tau, s.b, s.b2, s.y, s.w1, s.w2, s.w3, s.z, s.phs};
-  const int P = s.pitch;
-  typename C2<T>::type* M = s.M;
-  auto uk = [&](int k, int i) { return M[(size_t)(k + 1 + i) * P + k]; };
-  tail<T>(n, ref, tv, uk, *s.red, singular, ph, quality, tcoh, c, npairs);
-}
-
-// ----------------------------------------------------------------- FP32: one kernel
-template <int NB>
-__global__ void __launch_bounds__(kThreads, 2) fused_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
-                                                            int ref, float2* __restrict__ ph,
-                                                            float* __restrict__ quality, float* __restrict__ tcoh) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ GjShared<float, NB> gs;
-  const TriShared<float> s = tri_layout<float>(smem_raw, n);
-  const int tid = threadIdx.x, tx = tid >> 4, ty = tid & 15;
-  const int64_t npairs = (int64_t)n * (n - 1) / 2;
-  const int P = s.pitch;
-  for (int64_t pt = blockIdx.x; pt < n_pc; pt += gridDim.x) {
-    const float2* c = coh + pt * npairs;
-    float a[NB][NB];
-    unsigned used;
-    load_abs_gamma<float, NB>(a, used, c, n, tx, ty);
-    const bool singular = gj_tile<float, NB>(a, used, n, tx, ty, gs);
-    // M[kr][pc] = inv(|Gamma|)[kr][pc] * Gamma[kr][pc]
-#pragma unroll
-    for (int ib = 0; ib < NB; ++ib) {
-      const int r0 = ty + 16 * ib;
-      if (r0 >= n) continue;
-      const int kr = gs.step_of_row[r0];
-#pragma unroll
-      for (int jb = 0; jb < NB; ++jb) {
-        const int c0 = tx + 16 * jb;
-        if (c0 >= n) continue;
-        const int pc = gs.piv_of_step[c0];
-        float gx = 1.f, gy = 0.f;
-        if (kr != pc) {
-          const float2 g = c[kr < pc ? triu_index(kr, pc, n) : triu_index(pc, kr, n)];
-          gx = g.x;
-          gy = kr < pc ? g.y : -g.y;
-        }
-        s.M[(size_t)kr * P + pc] = make_float2(a[ib][jb] * gx, a[ib][jb] * gy);
-      }
-    }
-    __syncthreads();
-    tridiag_full<float>(s, n);
-    finish<float>(s, n, ref, singular, ph + pt * n, quality + pt, tcoh ? tcoh + pt : nullptr, c, npairs);
+struct PointWs {
+  size_t np, nq, bytes;
+  __host__ __device__ explicit PointWs(int n) {
+    using C = typename C2<T>::type;
+    np = (size_t)n * (n + 1) / 2;
+    nq = (size_t)n * (n - 1) / 2;
+    bytes = align16(np * sizeof(T)) + align16(nq * sizeof(C)) + align16(2 * (size_t)n * sizeof(T)) +
+            align16((size_t)n * sizeof(C));
   }
-}
+};
 
-// ----------------------------------------------------------------- FP64: two kernels
-template <int NB>
-__global__ void __launch_bounds__(kThreads, 1) inverse_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
-                                                             double* __restrict__ ainv, uint8_t* __restrict__ sing) {
-  __shared__ GjShared<double, NB> gs;
+template <typename T>
+struct PointPtr {
+  using C = typename C2<T>::type;
+  T* ainv;
+  C* refl;
+  T* d;
+  T* tau;
+  C* e;
+  __device__ PointPtr(unsigned char* ws, int64_t pt, int n) {
+    const PointWs<T> w(n);
+    unsigned char* b = ws + (size_t)pt * w.bytes;
+    ainv = reinterpret_cast<T*>(b);
+    b += align16(w.np * sizeof(T));
+    refl = reinterpret_cast<C*>(b);
+    b += align16(w.nq * sizeof(C));
+    d = reinterpret_cast<T*>(b);
+    tau = d + n;
+    b += align16(2 * (size_t)n * sizeof(T));
+    e = reinterpret_cast<C*>(b);
+  }
+};
+
+__host__ __device__ __forceinline__ size_t refl_off(int k, int n) { return (size_t)k * (n - 1) - (size_t)k * (k - 1) / 2; }
+
+// ----------------------------------------------------------------- kernel 1: inverse
+template <typename T, int NB>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) inverse_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
+                                                          unsigned char* __restrict__ ws, uint8_t* __restrict__ sing) {
+  __shared__ GjShared<T, NB> gs;
   const int tid = threadIdx.x, tx = tid >> 4, ty = tid & 15;
   const int64_t npairs = (int64_t)n * (n - 1) / 2;
-  const int64_t npk = (int64_t)n * (n + 1) / 2;
   for (int64_t pt = blockIdx.x; pt < n_pc; pt += gridDim.x) {
-    double a[NB][NB];
+    T a[NB][NB];
     unsigned used;
-    load_abs_gamma<double, NB>(a, used, coh + pt * npairs, n, tx, ty);
-    const bool singular = gj_tile<double, NB>(a, used, n, tx, ty, gs);
-    double* out = ainv + pt * npk;
+    load_abs_gamma<T, NB>(a, used, coh + pt * npairs, n, tx, ty);
+    const bool singular = gj_tile<T, NB>(a, used, n, tx, ty, gs);
+    T* out = PointPtr<T>(ws, pt, n).ainv;
 #pragma unroll
     for (int ib = 0; ib < NB; ++ib) {
       const int r0 = ty + 16 * ib;
@@ -445,78 +435,274 @@ __global__ void __launch_bounds__(kThreads, 1) inverse_kernel(const float2* __re
   }
 }
 
-__global__ void __launch_bounds__(kThreads) eig_kernel(const float2* __restrict__ coh, int64_t n_pc, int n, int ref,
-                                                       const double* __restrict__ ainv,
-                                                       const uint8_t* __restrict__ sing, float2* __restrict__ ph,
-                                                       float* __restrict__ quality, float* __restrict__ tcoh) {
+// ----------------------------------------------------------------- kernel 2: reduction
+template <typename T>
+__global__ void __launch_bounds__(kThreads) reduce_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
+                                                         unsigned char* __restrict__ ws) {
+  using C = typename C2<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const TriShared<double> s = tri_layout<double>(smem_raw, n);
+  const TriShared<T> s = tri_layout<T>(smem_raw, n);
   const int tid = threadIdx.x, nt = blockDim.x;
   const int64_t npairs = (int64_t)n * (n - 1) / 2;
-  const int64_t npk = (int64_t)n * (n + 1) / 2;
   const int P = s.pitch;
   for (int64_t pt = blockIdx.x; pt < n_pc; pt += gridDim.x) {
     const float2* c = coh + pt * npairs;
-    const double* ai = ainv + pt * npk;
-    for (int e = tid; e < n * n; e += nt) {
+    PointPtr<T> w(ws, pt, n);
+    for (int e = tid; e < n * n; e += nt) {  // M = inv(|Gamma|) o Gamma, full
       const int i = e / n, j = e - i * n;
       const int hi = max(i, j), lo = min(i, j);
-      double gx = 1.0, gy = 0.0;
+      T gx = 1, gy = 0;
       if (i != j) {
         const float2 g = c[triu_index(lo, hi, n)];
         gx = g.x;
         gy = i < j ? g.y : -g.y;
       }
-      const double sc = ai[(int64_t)hi * (hi + 1) / 2 + lo];
-      s.M[(size_t)i * P + j] = make_double2(sc * gx, sc * gy);
+      const T sc = w.ainv[(int64_t)hi * (hi + 1) / 2 + lo];
+      s.M[(size_t)i * P + j] = mk<T>(sc * gx, sc * gy);
     }
     __syncthreads();
-    tridiag_full<double>(s, n);
-    finish<double>(s, n, ref, sing[pt] != 0, ph + pt * n, quality + pt, tcoh ? tcoh + pt : nullptr, c, npairs);
+    tridiag_full<T>(s, n);
+    for (int i = tid; i < n; i += nt) {
+      w.d[i] = s.d[i];
+      w.tau[i] = (i + 2 < n) ? s.tau[i] : T(0);
+      if (i + 1 < n) w.e[i] = s.e[i];
+    }
+    for (int k = 0; k + 2 < n; ++k)  // reflector k: column k, rows k+1..n-1
+      for (int i = tid; i < n - k - 1; i += nt) w.refl[refl_off(k, n) + i] = s.M[(size_t)(k + 1 + i) * P + k];
+    __syncthreads();
   }
 }
 
-int sub_batch(int n) {
-  const size_t np = (size_t)n * (n + 1) / 2;
-  const size_t per = np * sizeof(double) + 1;
-  return (int)std::max<size_t>(1024, std::min<size_t>(65536, (size_t)(1ull << 30) / per));
+// ----------------------------------------------------------------- kernel 3: tail, one warp per point
+constexpr int kTailWarps = 8;
+
+template <typename T>
+__host__ __device__ inline size_t tail_warp_bytes(int n) {
+  using C = typename C2<T>::type;
+  return align16(6 * (size_t)n * sizeof(T)) + align16((size_t)n * sizeof(C)) + align16((size_t)n * sizeof(double2));
 }
 
+template <typename T>
+__global__ void __launch_bounds__(32 * kTailWarps) tail_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
+                                                              int ref, const unsigned char* __restrict__ ws,
+                                                              const uint8_t* __restrict__ sing,
+                                                              float2* __restrict__ ph, float* __restrict__ quality,
+                                                              float* __restrict__ tcoh) {
+  using C = typename C2<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned char* mine = smem_raw + (size_t)wid * tail_warp_bytes<T>(n);
+  T* d = reinterpret_cast<T*>(mine);
+  T* b = d + n;
+  T* b2 = b + n;
+  T* y = b2 + n;
+  T* w1 = y + n;
+  T* w2 = w1 + n;
+  C* z = reinterpret_cast<C*>(mine + align16(6 * (size_t)n * sizeof(T)));
+  double2* phs = reinterpret_cast<double2*>(mine + align16(6 * (size_t)n * sizeof(T)) + align16((size_t)n * sizeof(C)));
+  const int64_t npairs = (int64_t)n * (n - 1) / 2;
+  const float fnan = __int_as_float(0x7fffffff);
+  for (int64_t pt = (int64_t)blockIdx.x * kTailWarps + wid; pt < n_pc; pt += (int64_t)gridDim.x * kTailWarps) {
+    const PointPtr<T> w(const_cast<unsigned char*>(ws), pt, n);
+    // real tridiagonal: b = |e|, phases delta_{k+1} = delta_k e_k/|e_k| (warp prefix product)
+    C carry = mk<T>(1, 0);
+    for (int k0 = 0; k0 < n; k0 += 32) {
+      const int k = k0 + lane;
+      if (k < n) d[k] = w.d[k];
+      C f = mk<T>(1, 0);
+      if (k + 1 < n) {
+        const C ek = w.e[k];
+        const T a = sqrt(ek.x * ek.x + ek.y * ek.y);
+        b[k] = a;
+        b2[k] = a * a;
+        if (a > T(0)) f = mk<T>(ek.x / a, ek.y / a);
+      }
+      // inclusive scan of the factors f over the lanes
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const T ox = __shfl_up_sync(0xffffffffu, f.x, o), oy = __shfl_up_sync(0xffffffffu, f.y, o);
+        if (lane >= o) f = cmul_t(mk<T>(ox, oy), f);
+      }
+      const C dl = cmul_t(carry, f);  // delta_{k+1}
+      if (k0 == 0 && lane == 0) z[0] = mk<T>(1, 0);
+      if (k + 1 < n) z[k + 1] = dl;
+      carry = mk<T>(__shfl_sync(0xffffffffu, dl.x, 31), __shfl_sync(0xffffffffu, dl.y, 31));
+    }
+    __syncwarp();
+    // lambda_min by multisection
+    T lo = Lim<T>::huge(), hi = -Lim<T>::huge(), tnorm = 0;
+    for (int i = lane; i < n; i += 32) {
+      const T r = (i > 0 ? b[i - 1] : T(0)) + (i + 1 < n ? b[i] : T(0));
+      lo = fmin(lo, d[i] - r);
+      hi = fmax(hi, d[i] + r);
+      tnorm = fmax(tnorm, fabs(d[i]) + r);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+      tnorm = fmax(tnorm, __shfl_xor_sync(0xffffffffu, tnorm, o));
+    }
+    const T eps = Lim<T>::eps();
+    const T pivmin = fmax(Lim<T>::tiny(), eps * eps * tnorm * tnorm) + Lim<T>::tiny();
+    const T pad = T(2) * eps * fmax(tnorm, Lim<T>::tiny()) + T(2) * pivmin;
+    lo -= pad;
+    hi += pad;
+    for (int it = 0; it < 64; ++it) {
+      const T width = hi - lo;
+      if (!(width > T(2) * eps * fmax(fabs(lo), fabs(hi)) + T(4) * pivmin)) break;
+      const T sg = lo + width * (T)(lane + 1) / T(33);
+      const int cnt = sturm_count(d, b2, n, sg, pivmin);
+      const unsigned ball = __ballot_sync(0xffffffffu, cnt >= 1);
+      const int first = ball ? __ffs(ball) - 1 : 32;
+      const T nlo = (first == 0) ? lo : lo + width * (T)first / T(33);
+      const T nhi = (first == 32) ? hi : lo + width * (T)(first + 1) / T(33);
+      lo = nlo;
+      hi = nhi;
+    }
+    const T lam = T(0.5) * (lo + hi);
+    // eigenvector of the real tridiagonal by inverse iteration (lane 0)
+    for (int i = lane; i < n; i += 32) y[i] = T(1) + T(0.25) * (T)((i * 37) % 11) / T(11);
+    __syncwarp();
+    if (lane == 0) {
+      const T tiny = eps * fmax(tnorm, Lim<T>::tiny());
+      for (int it = 0; it < 2; ++it) {
+        tridiag_solve(d, b, n, lam, tiny, y, w1, w2, b2);  // b2 is free after the bisection
+        T sc = 0;
+        for (int i = 0; i < n; ++i) sc = fmax(sc, fabs(y[i]));
+        if (!(sc > T(0)) || !isfinite(sc)) break;
+        const T r = T(1) / sc;
+        for (int i = 0; i < n; ++i) y[i] *= r;
+      }
+    }
+    __syncwarp();
+    // v = Q D y
+    for (int i = lane; i < n; i += 32) { const C dl = z[i]; z[i] = mk<T>(dl.x * y[i], dl.y * y[i]); }
+    __syncwarp();
+    for (int k = n - 3; k >= 0; --k) {
+      const T tau = w.tau[k];
+      if (tau == T(0)) continue;
+      const C* u = w.refl + refl_off(k, n);
+      const int m = n - k - 1;
+      C sacc = mk<T>(0, 0);
+      C uu[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int i = lane + 32 * t;
+        uu[t] = mk<T>(0, 0);
+        if (i < m) {
+          uu[t] = u[i];
+          const C zi = z[k + 1 + i];
+          sacc.x += uu[t].x * zi.x + uu[t].y * zi.y;
+          sacc.y += uu[t].x * zi.y - uu[t].y * zi.x;
+        }
+      }
+      sacc.x = warp_sum(sacc.x);
+      sacc.y = warp_sum(sacc.y);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int i = lane + 32 * t;
+        if (i < m) {
+          const C tt = cmul_t(uu[t], sacc);
+          z[k + 1 + i].x -= tau * tt.x;
+          z[k + 1 + i].y -= tau * tt.y;
+        }
+      }
+      __syncwarp();
+    }
+    // normalise to the reference image
+    const bool singular = sing[pt] != 0;
+    const C zr = z[ref];
+    for (int i = lane; i < n; i += 32) {
+      const C v = cmulc_t(z[i], zr);
+      const double vx = v.x, vy = v.y, a = sqrt(vx * vx + vy * vy);
+      float2 o = make_float2((float)(vx / a), (float)(vy / a));
+      if (singular) o = make_float2(fnan, fnan);
+      ph[pt * n + i] = o;
+      phs[i] = make_double2(o.x, o.y);
+    }
+    if (lane == 0) quality[pt] = singular ? fnan : (float)lam;
+    __syncwarp();
+    if (tcoh) {  // |sum_q coh_q/|coh_q| conj(ph_m) ph_j| / n_pairs
+      const float2* c = coh + pt * npairs;
+      double tx = 0, ty = 0;
+      int mm = 0, jj = 1 + lane;
+      while (jj >= n && mm < n - 1) { mm += 1; jj = jj - n + mm + 1; }
+      for (int64_t q = lane; q < npairs; q += 32) {
+        const int m0 = mm, j0 = jj;
+        jj += 32;
+        while (jj >= n && mm < n - 1) { mm += 1; jj = jj - n + mm + 1; }
+        const float2 g = c[q];
+        const double ga = sqrt((double)g.x * g.x + (double)g.y * g.y);
+        const double2 v = cmul(make_double2(g.x / ga, g.y / ga), cmulc(phs[j0], phs[m0]));
+        tx += v.x;
+        ty += v.y;
+      }
+      tx = warp_sum(tx);
+      ty = warp_sum(ty);
+      if (lane == 0) tcoh[pt] = (float)(sqrt(tx * tx + ty * ty) / (double)npairs);
+    }
+    __syncwarp();
+  }
+}
+
+// ----------------------------------------------------------------- host side
 template <class K>
-int occupancy(K kernel, size_t smem) {
+int occupancy(K kernel, int threads, size_t smem) {
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kThreads, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess) return 0;
   return occ;
 }
 
-template <int NB>
-int launch_fused(const float2* coh, int64_t n_pc, int n, int ref, float2* ph, float* q, float* t, cudaStream_t s) {
-  const size_t smem = tri_bytes<float>(n);
-  MR_CUDA_TRY(cudaFuncSetAttribute(fused_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int occ = occupancy(fused_kernel<NB>, smem);
-  if (occ < 1) return fail(MR_ERR_UNSUPPORTED, "emi: %zu bytes of shared memory per CTA do not fit", smem);
-  const int64_t grid = std::min<int64_t>(n_pc, (int64_t)sm_count() * occ);
-  fused_kernel<NB><<<(unsigned)grid, kThreads, smem, s>>>(coh, n_pc, n, ref, ph, q, t);
-  return check_launch("emi (fp32)");
+template <typename T>
+int sub_batch(int n) {
+  const PointWs<T> w(n);
+  return (int)std::max<size_t>(1024, std::min<size_t>(1 << 17, (size_t)(1ull << 30) / (w.bytes + 1)));
 }
 
-template <int NB>
-int launch_inverse(const float2* coh, int64_t n, int nimg, double* ainv, uint8_t* sing, cudaStream_t s) {
-  const int occ = std::max(1, occupancy(inverse_kernel<NB>, 0));
-  const int64_t grid = std::min<int64_t>(n, (int64_t)sm_count() * occ);
-  inverse_kernel<NB><<<(unsigned)grid, kThreads, 0, s>>>(coh, n, nimg, ainv, sing);
-  return check_launch("emi inverse (fp64)");
-}
-
-int launch_eig64(const float2* c, int64_t nb, int n, int ref, const double* ainv, const uint8_t* sing, float2* ph,
-                 float* quality, float* tcoh, cudaStream_t s) {
-  const size_t smem = tri_bytes<double>(n);
-  MR_CUDA_TRY(cudaFuncSetAttribute(eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int occ = occupancy(eig_kernel, smem);
-  if (occ < 1) return fail(MR_ERR_UNSUPPORTED, "emi: %zu bytes of shared memory per CTA do not fit", smem);
+template <typename T, int NB>
+int launch_inverse(const float2* coh, int64_t nb, int n, unsigned char* ws, uint8_t* sing, cudaStream_t s) {
+  const int occ = std::max(1, occupancy(inverse_kernel<T, NB>, kThreads, 0));
   const int64_t grid = std::min<int64_t>(nb, (int64_t)sm_count() * occ);
-  eig_kernel<<<(unsigned)grid, kThreads, smem, s>>>(c, nb, n, ref, ainv, sing, ph, quality, tcoh);
-  return check_launch("emi eig (fp64)");
+  inverse_kernel<T, NB><<<(unsigned)grid, kThreads, 0, s>>>(coh, nb, n, ws, sing);
+  return check_launch("emi inverse");
+}
+
+template <typename T>
+int run_precision(const float2* coh, int64_t n_pc, int n, int ref, float2* ph, float* quality, float* tcoh,
+                  unsigned char* ws, cudaStream_t s) {
+  const int64_t sub = std::min<int64_t>(n_pc, sub_batch<T>(n));
+  uint8_t* sing = ws + align16((size_t)sub * PointWs<T>(n).bytes);
+  const size_t rsmem = tri_bytes<T>(n);
+  MR_CUDA_TRY(cudaFuncSetAttribute(reduce_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
+  const int rocc = occupancy(reduce_kernel<T>, kThreads, rsmem);
+  if (rocc < 1) return fail(MR_ERR_UNSUPPORTED, "emi: %zu bytes of shared memory per CTA do not fit", rsmem);
+  const size_t tsmem = kTailWarps * tail_warp_bytes<T>(n);
+  MR_CUDA_TRY(cudaFuncSetAttribute(tail_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
+  const int tocc = std::max(1, occupancy(tail_kernel<T>, 32 * kTailWarps, tsmem));
+  const int64_t npairs = (int64_t)n * (n - 1) / 2;
+  for (int64_t b0 = 0; b0 < n_pc; b0 += sub) {
+    const int64_t nb = std::min<int64_t>(sub, n_pc - b0);
+    const float2* c = coh + b0 * npairs;
+    int rc;
+    switch ((n + 15) / 16) {
+      case 1: case 2: rc = launch_inverse<T, 2>(c, nb, n, ws, sing, s); break;
+      case 3: rc = launch_inverse<T, 3>(c, nb, n, ws, sing, s); break;
+      case 4: rc = launch_inverse<T, 4>(c, nb, n, ws, sing, s); break;
+      case 5: rc = launch_inverse<T, 5>(c, nb, n, ws, sing, s); break;
+      case 6: rc = launch_inverse<T, 6>(c, nb, n, ws, sing, s); break;
+      case 7: rc = launch_inverse<T, 7>(c, nb, n, ws, sing, s); break;
+      default: rc = launch_inverse<T, 8>(c, nb, n, ws, sing, s); break;
+    }
+    if (rc) return rc;
+    reduce_kernel<T><<<(unsigned)std::min<int64_t>(nb, (int64_t)sm_count() * rocc), kThreads, rsmem, s>>>(c, nb, n, ws);
+    if (int e = check_launch("emi reduce")) return e;
+    const int64_t tgrid = std::min<int64_t>((nb + kTailWarps - 1) / kTailWarps, (int64_t)sm_count() * tocc);
+    tail_kernel<T><<<(unsigned)tgrid, 32 * kTailWarps, tsmem, s>>>(c, nb, n, ref, ws, sing, ph + b0 * n,
+                                                                    quality + b0, tcoh ? tcoh + b0 : nullptr);
+    if (int e = check_launch("emi tail")) return e;
+  }
+  return MR_OK;
 }
 
 }  // namespace
@@ -524,48 +710,18 @@ int launch_eig64(const float2* c, int64_t nb, int n, int ref, const double* ainv
 int fast_supported(int n) { return n >= 2 && n <= kMaxFastN; }
 
 size_t fast_workspace_bytes(int64_t n_pc, int n) {
-  const int64_t sub = std::min<int64_t>(n_pc, sub_batch(n));
-  const size_t np = (size_t)n * (n + 1) / 2;
-  return ((size_t)sub * np * sizeof(double) + 255) / 256 * 256 + (size_t)sub;
+  const int64_t s32 = std::min<int64_t>(n_pc, sub_batch<float>(n));
+  const int64_t s64 = std::min<int64_t>(n_pc, sub_batch<double>(n));
+  return std::max(align16((size_t)s32 * PointWs<float>(n).bytes) + (size_t)s32,
+                  align16((size_t)s64 * PointWs<double>(n).bytes) + (size_t)s64);
 }
 
 int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, float2* ph, float* quality,
              float* tcoh, void* workspace, size_t workspace_bytes, cudaStream_t s) {
   (void)workspace_bytes;
-  if (precision != MR_PREC_FP64) {
-    switch ((n + 15) / 16) {
-      case 1: case 2: return launch_fused<2>(coh, n_pc, n, ref, ph, quality, tcoh, s);
-      case 3: return launch_fused<3>(coh, n_pc, n, ref, ph, quality, tcoh, s);
-      case 4: return launch_fused<4>(coh, n_pc, n, ref, ph, quality, tcoh, s);
-      case 5: return launch_fused<5>(coh, n_pc, n, ref, ph, quality, tcoh, s);
-      case 6: return launch_fused<6>(coh, n_pc, n, ref, ph, quality, tcoh, s);
-      case 7: return launch_fused<7>(coh, n_pc, n, ref, ph, quality, tcoh, s);
-      default: return launch_fused<8>(coh, n_pc, n, ref, ph, quality, tcoh, s);
-    }
-  }
-  const int64_t sub = std::min<int64_t>(n_pc, sub_batch(n));
-  const size_t np = (size_t)n * (n + 1) / 2;
-  double* ainv = static_cast<double*>(workspace);
-  uint8_t* sing = static_cast<uint8_t*>(workspace) + ((size_t)sub * np * sizeof(double) + 255) / 256 * 256;
-  const int64_t npairs = (int64_t)n * (n - 1) / 2;
-  for (int64_t b0 = 0; b0 < n_pc; b0 += sub) {
-    const int64_t nb = std::min<int64_t>(sub, n_pc - b0);
-    const float2* c = coh + b0 * npairs;
-    int rc;
-    switch ((n + 15) / 16) {
-      case 1: case 2: rc = launch_inverse<2>(c, nb, n, ainv, sing, s); break;
-      case 3: rc = launch_inverse<3>(c, nb, n, ainv, sing, s); break;
-      case 4: rc = launch_inverse<4>(c, nb, n, ainv, sing, s); break;
-      case 5: rc = launch_inverse<5>(c, nb, n, ainv, sing, s); break;
-      case 6: rc = launch_inverse<6>(c, nb, n, ainv, sing, s); break;
-      case 7: rc = launch_inverse<7>(c, nb, n, ainv, sing, s); break;
-      default: rc = launch_inverse<8>(c, nb, n, ainv, sing, s); break;
-    }
-    if (rc) return rc;
-    rc = launch_eig64(c, nb, n, ref, ainv, sing, ph + b0 * n, quality + b0, tcoh ? tcoh + b0 : nullptr, s);
-    if (rc) return rc;
-  }
-  return MR_OK;
+  auto* ws = static_cast<unsigned char*>(workspace);
+  if (precision == MR_PREC_FP64) return run_precision<double>(coh, n_pc, n, ref, ph, quality, tcoh, ws, s);
+  return run_precision<float>(coh, n_pc, n, ref, ph, quality, tcoh, ws, s);
 }
 
 }  // namespace emi
