@@ -102,6 +102,22 @@ int mr_ds_extract(const int32_t* shp_num, const uint8_t* is_shp, int nlines, int
                   int win, int min_shp, int32_t* idx, uint8_t* pc_is_shp, int64_t max_ds,
                   int64_t* n_ds, void* workspace, size_t workspace_bytes, mr_stream_t stream);
 
+/* Allocation-free variant of mr_ds_extract. This entry point has no counterpart in the
+ * reference; it exists for callers that cannot provide device workspace memory (a host
+ * that plans every device byte up front, a plugin that must not bypass its host
+ * framework's allocator, a binding with no route to a device allocator). Same arguments
+ * and results as mr_ds_extract without the workspace: the per-block counts live in a
+ * fixed array inside the library (128 KiB per device, held until the process exits), so
+ * rasters are limited to MR_DS_EXTRACT_NOALLOC_MAX_PIXELS pixels (larger ones return
+ * MR_ERR_UNSUPPORTED). It calls no allocator. The first call on a device looks up that
+ * array's device address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. Every call shares the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race on it, so serialise them. */
+#define MR_DS_EXTRACT_NOALLOC_MAX_PIXELS (16384LL * 1024LL)
+int mr_ds_extract_noalloc(const int32_t* shp_num, const uint8_t* is_shp, int nlines, int width,
+                          int win, int min_shp, int32_t* idx, uint8_t* pc_is_shp, int64_t max_ds,
+                          int64_t* n_ds, mr_stream_t stream);
+
 /* ---------------------------------------------------------------- coherence
  * Replaces moraine.co.emperical_co_pc (moraine/co.py:230-266; kernel :141-190, CPU
  * :194-227): coh[i, q] = sum_s z_m conj(z_j) / sqrt(sum_s |z_m|^2 * sum_s |z_j|^2) over

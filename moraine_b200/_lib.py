@@ -32,6 +32,7 @@ _SIGNATURES = {
     "mr_select_shp": (c_int, [P, c_int64, c_int, c_double, P, P, P]),
     "mr_ds_extract_workspace_bytes": (c_size_t, [c_int64]),
     "mr_ds_extract": (c_int, [P, P, c_int, c_int, c_int, c_int, P, P, c_int64, P, P, c_size_t, P]),
+    "mr_ds_extract_noalloc": (c_int, [P, P, c_int, c_int, c_int, c_int, P, P, c_int64, P, P]),
     "mr_emperical_co_pc": (c_int, [P, c_int, c_int, c_int, P, c_int64, P, c_int, c_int, c_int, P, c_int, P,
                                    c_int, P]),
     "mr_emperical_co": (c_int, [P, c_int, c_int, c_int, P, c_int, c_int, P, P, P]),

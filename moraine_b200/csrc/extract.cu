@@ -147,3 +147,75 @@ extern "C" int mr_ds_extract(const int32_t* shp_num, const uint8_t* is_shp, int 
                                                         counts, idx, pc_is_shp, max_ds);
   return check_launch("ds_extract");
 }
+
+// ------------------------------------------------------------------------------------
+// Allocation-free variant.
+//
+// Some callers cannot hand this library a device workspace: a host that owns every
+// byte of device memory up front (a fixed-budget tile server, a plugin inside another
+// framework's process whose allocator must not be bypassed) or a binding from a language
+// with no route to a device allocator. For them mr_ds_extract_noalloc keeps its per-block
+// counts in a fixed array compiled into this library instead of a caller workspace.
+//
+// The array below lives in every GPU that loads the library until the process exits
+// (kNoAllocMaxBlocks * 8 bytes = 128 KiB per device). Its address is a device address,
+// which host code must look up per device (cudaGetSymbolAddress) before passing it to a
+// kernel: the symbol's name in host code is only a host-side stand-in.
+#include <mutex>
+
+namespace mr {
+namespace {
+
+constexpr int64_t kNoAllocMaxBlocks = 16384;  // rasters up to 16384 * 1024 = 16,777,216 pixels
+static __device__ __align__(256) int64_t g_extract_counts[kNoAllocMaxBlocks];
+
+// Device address of g_extract_counts on the current device, looked up once per device.
+int noalloc_counts(int64_t** out) {
+  static std::mutex mu;
+  static int64_t* addr[64] = {nullptr};
+  int dev = 0;
+  MR_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(MR_ERR_UNSUPPORTED, "ds_extract_noalloc: device index %d", dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (addr[dev] == nullptr) {
+    void* p = nullptr;
+    MR_CUDA_TRY(cudaGetSymbolAddress(&p, g_extract_counts));
+    addr[dev] = static_cast<int64_t*>(p);
+  }
+  *out = addr[dev];
+  return MR_OK;
+}
+
+}  // namespace
+}  // namespace mr
+
+extern "C" int mr_ds_extract_noalloc(const int32_t* shp_num, const uint8_t* is_shp, int nlines, int width, int win,
+                                     int min_shp, int32_t* idx, uint8_t* pc_is_shp, int64_t max_ds, int64_t* n_ds,
+                                     mr_stream_t stream) {
+  MR_REQUIRE(shp_num && n_ds, "ds_extract_noalloc: NULL shp_num or n_ds");
+  MR_REQUIRE(nlines >= 0 && width >= 0 && win > 0, "ds_extract_noalloc: bad shape");
+  MR_REQUIRE(max_ds >= 0, "ds_extract_noalloc: negative max_ds");
+  MR_REQUIRE(pc_is_shp == nullptr || is_shp != nullptr, "ds_extract_noalloc: pc_is_shp needs is_shp");
+  MR_REQUIRE(max_ds == 0 || idx != nullptr, "ds_extract_noalloc: idx is NULL");
+  const int64_t npix = (int64_t)nlines * width;
+  const int64_t nblocks = (npix + kBlk - 1) / kBlk;
+  if (nblocks > kNoAllocMaxBlocks)
+    return fail(MR_ERR_UNSUPPORTED,
+                "ds_extract_noalloc: raster of %lld pixels exceeds the %lld-pixel limit of the allocation-free "
+                "variant; use mr_ds_extract with a workspace",
+                (long long)npix, (long long)(kNoAllocMaxBlocks * kBlk));
+  cudaStream_t s = as_stream(stream);
+  if (npix == 0) {
+    MR_CUDA_TRY(cudaMemsetAsync(n_ds, 0, sizeof(int64_t), s));
+    return MR_OK;
+  }
+  int64_t* counts = nullptr;
+  if (int rc = noalloc_counts(&counts)) return rc;
+  // count_kernel overwrites counts[0, nblocks) before anything reads them, so what an
+  // earlier call left in the array never leaks into this one
+  count_kernel<<<(unsigned)nblocks, kThreads, 0, s>>>(shp_num, npix, min_shp, counts);
+  scan_kernel<<<1, 1024, 0, s>>>(counts, nblocks, n_ds);
+  scatter_kernel<<<(unsigned)nblocks, kThreads, 0, s>>>(shp_num, is_shp, npix, width, win, min_shp, counts, idx,
+                                                        pc_is_shp, max_ds);
+  return check_launch("ds_extract_noalloc");
+}
