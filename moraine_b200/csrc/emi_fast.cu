@@ -9,9 +9,7 @@
 // Householder reduction (tridiag_full): M = inv(|Gamma|) o Gamma in full Hermitian storage
 //   in shared memory (odd row pitch). Step k's rank-2 update is fused with the product of
 //   step k+1: a pair of threads owns each row of the trailing block, updates it and
-//   accumulates (M u)_i, so no cross-lane reduction is needed beyond the pair. Warp 0
-//   finishes step k-1 and forms reflector k in shared vectors between the two barriers of
-//   each step.
+//   accumulates (M u)_i, so no cross-lane reduction is needed beyond the pair.
 // Three kernels per sub-batch of points, in FP32 or FP64 (template T):
 //   inverse_kernel<T, NB>  inv(|Gamma|) in registers -> workspace (lower triangle, packed);
 //   reduce_kernel<T>       M in shared memory, Householder reduction -> workspace (d, e, tau,
@@ -62,67 +60,47 @@ __device__ __forceinline__ void load_abs_gamma(T (&a)[NB][NB], unsigned& used, c
   }
 }
 
-// a[ib][kb] for a CTA-uniform kb (a switch instead of per-element selects).
-template <typename T, int NB>
-__device__ __forceinline__ T col_of(const T (&a)[NB][NB], int ib, int kb) {
-  T v = 0;
-  switch (kb) {
-    case 0: v = a[ib][0]; break;
-    case 1: if (NB > 1) v = a[ib][1 < NB ? 1 : 0]; break;
-    case 2: if (NB > 2) v = a[ib][2 < NB ? 2 : 0]; break;
-    case 3: if (NB > 3) v = a[ib][3 < NB ? 3 : 0]; break;
-    case 4: if (NB > 4) v = a[ib][4 < NB ? 4 : 0]; break;
-    case 5: if (NB > 5) v = a[ib][5 < NB ? 5 : 0]; break;
-    case 6: if (NB > 6) v = a[ib][6 < NB ? 6 : 0]; break;
-    default: if (NB > 7) v = a[ib][7 < NB ? 7 : 0]; break;
-  }
-  return v;
-}
+__device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double recip(double x) { return 1.0 / x; }
 
+// One Gauss-Jordan step k = 16 KB + kt on the register tile; KB is a compile-time column
+// slot, so the pivot column is read and rewritten without dynamic register indexing.
 template <typename T, int NB, int KB>
-__device__ __forceinline__ void set_col(T (&a)[NB][NB], int ib, T v) {
-  if (KB < NB) a[ib][KB < NB ? KB : 0] = v;
-}
-
-// In-place Gauss-Jordan inverse with partial pivoting on the register tile. Returns true
-// when a zero pivot was met (the matrix is singular).
-template <typename T, int NB>
-__device__ bool gj_tile(T (&a)[NB][NB], unsigned used, int n, int tx, int ty, GjShared<T, NB>& s) {
+__device__ __forceinline__ void gj_step(T (&a)[NB][NB], unsigned& used, int k, int tx, int ty, bool& singular,
+                                        GjShared<T, NB>& s) {
   const int tid = threadIdx.x;
-  const unsigned half = (tx & 1) ? 0xFFFF0000u : 0x0000FFFFu;
-  bool singular = false;
-  for (int k = 0; k < n; ++k) {
-    const int buf = k & 1, kb = k >> 4;
-    const bool owner = tx == (k & 15);
-    if (owner) {  // the half-warp owning column k: publish it, find the pivot
-      T best = T(-1);
-      int bi = -1;
+  const int buf = k & 1;
+  const bool owner = tx == (k & 15);
+  if (owner) {  // the half-warp owning column k: publish it, find the pivot
+    const unsigned half = (tx & 1) ? 0xFFFF0000u : 0x0000FFFFu;
+    T best = T(-1);
+    int bi = -1;
 #pragma unroll
-      for (int ib = 0; ib < NB; ++ib) {
-        const T v = col_of<T, NB>(a, ib, kb);
-        s.col[buf][ty + 16 * ib] = v;
-        const T av = fabs(v);
-        if (!(used & (1u << ib)) && av > best) { best = av; bi = ty + 16 * ib; }
-      }
-#pragma unroll
-      for (int o = 8; o > 0; o >>= 1) {
-        const T ob = __shfl_xor_sync(half, best, o, 16);
-        const int oi = __shfl_xor_sync(half, bi, o, 16);
-        if (ob > best || (ob == best && oi >= 0 && (bi < 0 || oi < bi))) { best = ob; bi = oi; }
-      }
-      if (ty == 0) s.piv[buf] = bi;
+    for (int ib = 0; ib < NB; ++ib) {
+      const T v = a[ib][KB];
+      s.col[buf][ty + 16 * ib] = v;
+      const T av = fabs(v);
+      if (!(used & (1u << ib)) && av > best) { best = av; bi = ty + 16 * ib; }
     }
-    __syncthreads();
-    const int p = s.piv[buf];
-    T pv = s.col[buf][p];
-    if (pv == T(0)) { singular = true; pv = T(1); }
-    const T rp = T(1) / pv;
-    if (ty == (p & 15)) used |= 1u << (p >> 4);
-    if (tid == 0) { s.piv_of_step[k] = p; s.step_of_row[p] = k; }
-    const int pl = p & 15;
-    // pivot row (scaled) from row lane pl of this column group; p >> 4 is CTA-uniform
-    T r[NB];
-    switch (p >> 4) {
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+      const T ob = __shfl_xor_sync(half, best, o, 16);
+      const int oi = __shfl_xor_sync(half, bi, o, 16);
+      if (ob > best || (ob == best && oi >= 0 && (bi < 0 || oi < bi))) { best = ob; bi = oi; }
+    }
+    if (ty == 0) s.piv[buf] = bi;
+  }
+  __syncthreads();
+  const int p = s.piv[buf];
+  T pv = s.col[buf][p];
+  if (pv == T(0)) { singular = true; pv = T(1); }
+  const T rp = recip(pv);
+  if (ty == (p & 15)) used |= 1u << (p >> 4);
+  if (tid == 0) { s.piv_of_step[k] = p; s.step_of_row[p] = k; }
+  const int pl = p & 15;
+  // pivot row (scaled) from row lane pl of this column group; p >> 4 is CTA-uniform
+  T r[NB];
+  switch (p >> 4) {
 #define MR_GJ_ROW(PB)                                                                  \
   case PB:                                                                             \
     if (PB < NB) {                                                                     \
@@ -130,33 +108,42 @@ __device__ bool gj_tile(T (&a)[NB][NB], unsigned used, int n, int tx, int ty, Gj
           __shfl_sync(0xffffffffu, a[PB < NB ? PB : 0][jb], pl, 16) * rp;              \
     }                                                                                  \
     break;
-      MR_GJ_ROW(0) MR_GJ_ROW(1) MR_GJ_ROW(2) MR_GJ_ROW(3) MR_GJ_ROW(4) MR_GJ_ROW(5) MR_GJ_ROW(6)
-      default: MR_GJ_ROW(7)
+    MR_GJ_ROW(0) MR_GJ_ROW(1) MR_GJ_ROW(2) MR_GJ_ROW(3) MR_GJ_ROW(4) MR_GJ_ROW(5) MR_GJ_ROW(6)
+    default: MR_GJ_ROW(7)
 #undef MR_GJ_ROW
-    }
-    // a -= f_i r_j everywhere, with f_p = pv - 1 so that the pivot row becomes r
+  }
+  // a -= f_i r_j everywhere, with f_p = pv - 1 so that the pivot row becomes r; then
+  // column k becomes delta_ip / pv - f_i / pv
 #pragma unroll
-    for (int ib = 0; ib < NB; ++ib) {
-      const int i = ty + 16 * ib;
-      const T f = (i == p) ? pv - T(1) : s.col[buf][i];
+  for (int ib = 0; ib < NB; ++ib) {
+    const int i = ty + 16 * ib;
+    const T fi = s.col[buf][i];
+    const T f = (i == p) ? pv - T(1) : fi;
 #pragma unroll
-      for (int jb = 0; jb < NB; ++jb) a[ib][jb] -= f * r[jb];
-    }
-    if (owner) {  // column k: delta_ip - f_i / pv
+    for (int jb = 0; jb < NB; ++jb) a[ib][jb] -= f * r[jb];
+    if (owner) a[ib][KB] = (i == p) ? rp : -fi * rp;
+  }
+}
+
+// In-place Gauss-Jordan inverse with partial pivoting on the register tile. Returns true
+// when a zero pivot was met (the matrix is singular).
+template <typename T, int NB>
+__device__ bool gj_tile(T (&a)[NB][NB], unsigned used, int n, int tx, int ty, GjShared<T, NB>& s) {
+  bool singular = false;
 #pragma unroll
-      for (int ib = 0; ib < NB; ++ib) {
-        const int i = ty + 16 * ib;
-        const T v = (i == p) ? rp : -s.col[buf][i] * rp;
-        switch (kb) {
-          case 0: set_col<T, NB, 0>(a, ib, v); break;
-          case 1: set_col<T, NB, 1>(a, ib, v); break;
-          case 2: set_col<T, NB, 2>(a, ib, v); break;
-          case 3: set_col<T, NB, 3>(a, ib, v); break;
-          case 4: set_col<T, NB, 4>(a, ib, v); break;
-          case 5: set_col<T, NB, 5>(a, ib, v); break;
-          case 6: set_col<T, NB, 6>(a, ib, v); break;
-          default: set_col<T, NB, 7>(a, ib, v); break;
-        }
+  for (int kb = 0; kb < NB; ++kb) {
+    for (int kt = 0; kt < 16; ++kt) {
+      const int k = 16 * kb + kt;
+      if (k >= n) break;
+      switch (kb) {  // compile-time slot (the loop over kb is unrolled)
+        case 0: gj_step<T, NB, 0>(a, used, k, tx, ty, singular, s); break;
+        case 1: if (NB > 1) gj_step<T, NB, (1 < NB ? 1 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 2: if (NB > 2) gj_step<T, NB, (2 < NB ? 2 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 3: if (NB > 3) gj_step<T, NB, (3 < NB ? 3 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 4: if (NB > 4) gj_step<T, NB, (4 < NB ? 4 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 5: if (NB > 5) gj_step<T, NB, (5 < NB ? 5 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 6: if (NB > 6) gj_step<T, NB, (6 < NB ? 6 : 0)>(a, used, k, tx, ty, singular, s); break;
+        default: if (NB > 7) gj_step<T, NB, (7 < NB ? 7 : 0)>(a, used, k, tx, ty, singular, s); break;
       }
     }
   }
@@ -238,7 +225,11 @@ template <typename C> __device__ __forceinline__ void rank2(C& a, C ui, C wj, C 
 }
 
 // Householder reduction of the Hermitian M (full storage in s.M) to tridiagonal (s.d, s.e),
-// reflector k stored in column k (rows k+1..n-1) with scalar s.tau[k]. Whole CTA.
+// reflector k stored in column k (rows k+1..n-1) with scalar s.tau[k]. Whole CTA, two
+// barriers per step: warp 0 finishes step k-1 and forms reflector k from column k brought
+// up to date, x_i = A_i + K B_i (A_i, B_i from the same pass as the dot product that gives
+// K = tau/2 u^H p, so one load pass and two warp reductions); then a thread pair per row
+// applies step k-1's update to the row and accumulates (M u_k)_i.
 template <typename T>
 __device__ void tridiag_full(const TriShared<T>& s, int n) {
   using C = typename C2<T>::type;
@@ -250,33 +241,44 @@ __device__ void tridiag_full(const TriShared<T>& s, int n) {
   for (int k = 0; k + 2 < n; ++k) {
     C* up = s.vec + ((k + 1) & 1) * n;  // u_{k-1}
     C* uc = s.vec + (k & 1) * n;        // u_k
-    // ---- warp 0: w_{k-1} = p - K u_{k-1}; column k up to date; reflector k
+    // ---- warp 0: finish step k-1 and form reflector k
     if (wid == 0) {
       const T tau_prev = k > 0 ? s.tau[k - 1] : T(0);
       const bool pending = tau_prev != T(0);
-      if (pending) {
-        const C* p = s.pv + ((k + 1) & 1) * n;
-        T dot = 0;
-        for (int i = k + lane; i < n; i += 32) {
-          const C pi = p[i], ui = up[i];
-          wp[i] = pi;
-          dot += ui.x * pi.x + ui.y * pi.y;
+      const C* p = s.pv + ((k + 1) & 1) * n;
+      C A[4], B[4], pp[4], uu[4];
+      T dot = 0;
+      C pk = mk<T>(0, 0), ukk = mk<T>(0, 0);
+      if (pending) { pk = p[k]; ukk = up[k]; }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int i = k + lane + 32 * t;
+        A[t] = B[t] = pp[t] = uu[t] = mk<T>(0, 0);
+        if (i < n) {
+          A[t] = M[(size_t)i * P + k];
+          if (pending) {
+            pp[t] = p[i];
+            uu[t] = up[i];
+            dot += uu[t].x * pp[t].x + uu[t].y * pp[t].y;
+            // x_i = a_ik - u_i conj(w_k) - w_i conj(u_k) = A_i + K B_i, w = p - K u
+            rank2(A[t], uu[t], pk, pp[t], ukk);
+            B[t] = mk<T>(2 * (uu[t].x * ukk.x + uu[t].y * ukk.y), 2 * (uu[t].y * ukk.x - uu[t].x * ukk.y));
+            if (i > k) M[(size_t)i * P + k - 1] = uu[t];  // reflector k-1 (rows >= k) kept in column k-1
+          }
         }
-        const T K = T(0.5) * tau_prev * warp_sum(dot);
-        for (int i = k + lane; i < n; i += 32) { wp[i].x -= K * up[i].x; wp[i].y -= K * up[i].y; }
-        __syncwarp();
       }
-      C ukk = mk<T>(0, 0), wkk = mk<T>(0, 0);
-      if (pending) { ukk = up[k]; wkk = wp[k]; }
+      if (pending && lane == 0) M[(size_t)k * P + k - 1] = ukk;
+      const T K = pending ? T(0.5) * tau_prev * warp_sum(dot) : T(0);
       T xn2 = 0;
-      for (int i = k + lane; i < n; i += 32) {
-        C x = M[(size_t)i * P + k];
-        if (pending) {
-          rank2(x, up[i], wkk, wp[i], ukk);
-          M[(size_t)i * P + k - 1] = up[i];  // reflector k-1 (rows >= k) into column k-1
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int i = k + lane + 32 * t;
+        if (i < n) {
+          const C x = mk<T>(A[t].x + K * B[t].x, A[t].y + K * B[t].y);
+          if (pending) wp[i] = mk<T>(pp[t].x - K * uu[t].x, pp[t].y - K * uu[t].y);
+          uc[i] = x;
+          if (i >= k + 2) xn2 += x.x * x.x + x.y * x.y;
         }
-        uc[i] = x;
-        if (i >= k + 2) xn2 += x.x * x.x + x.y * x.y;
       }
       xn2 = warp_sum(xn2);
       __syncwarp();
@@ -406,7 +408,7 @@ __host__ __device__ __forceinline__ size_t refl_off(int k, int n) { return (size
 
 // ----------------------------------------------------------------- kernel 1: inverse
 template <typename T, int NB>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) inverse_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
+__global__ void __launch_bounds__(kThreads, 1) inverse_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
                                                           unsigned char* __restrict__ ws, uint8_t* __restrict__ sing) {
   __shared__ GjShared<T, NB> gs;
   const int tid = threadIdx.x, tx = tid >> 4, ty = tid & 15;
