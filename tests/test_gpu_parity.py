@@ -80,7 +80,7 @@ def test_co_pc_matches_reference_fixture(cuda, golden):
     np.testing.assert_array_equal(mb.uncompress_coh(g["coh"]), O.uncompress_coh(g["coh"]))
 
 
-@pytest.mark.parametrize("precision,tol", [("fp32", 2e-6), ("fp64", 1e-7)])
+@pytest.mark.parametrize("precision,tol", [("fp32", 2e-6), ("fp64", 1e-7), ("bf16x3", 3e-5), ("bf16", 1.5e-2)])
 @pytest.mark.parametrize("name,size", [("c0", 64), ("c1", 48), ("c2", 48), ("c3", 24)])
 def test_co_pc_vs_oracle(cuda, name, size, precision, tol):
     cfg = CONFIGS[name].scaled(nlines=size, width=size)
@@ -89,6 +89,10 @@ def test_co_pc_vs_oracle(cuda, name, size, precision, tol):
     is_shp, num = O.select_shp(p, cfg.p_max)
     idx, pc = O.ds_candidates(is_shp, num, 1)
     ref = O.emperical_co_pc(z, idx, pc)
+    if precision.startswith("bf16") and cfg.nimages > 128:
+        with pytest.raises(NotImplementedError):
+            mb.emperical_co_pc(z, idx, pc, precision=precision)
+        return
     coh = mb.emperical_co_pc(z, idx, pc, precision=precision)
     assert np.abs(coh - ref).max() < tol
 
