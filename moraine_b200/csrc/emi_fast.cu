@@ -6,10 +6,9 @@
 //   p_k among the rows not yet used (largest |a|) and publishes column k through a
 //   double-buffered shared vector; every column group fetches row p_k by shuffles. One
 //   barrier per step. The result R satisfies inv[k][p_j] = R[p_k][j].
-// Householder reduction (tridiag_full): M = inv(|Gamma|) o Gamma in full Hermitian storage
-//   in shared memory (odd row pitch). Step k's rank-2 update is fused with the product of
-//   step k+1: a pair of threads owns each row of the trailing block, updates it and
-//   accumulates (M u)_i, so no cross-lane reduction is needed beyond the pair.
+// Householder reduction (tridiag_packed): M = inv(|Gamma|) o Gamma as a packed lower
+//   triangle in shared memory; step k's rank-2 update is fused with the product of step
+//   k+1, mirrored row pairs give every thread the same work.
 // Three kernels per sub-batch of points, in FP32 or FP64 (template T):
 //   inverse_kernel<T, NB>  inv(|Gamma|) in registers -> workspace (lower triangle, packed);
 //   reduce_kernel<T>       M in shared memory, Householder reduction -> workspace (d, e, tau,
@@ -151,12 +150,11 @@ __device__ bool gj_tile(T (&a)[NB][NB], unsigned used, int n, int tx, int ty, Gj
   return singular;
 }
 
-// ----------------------------------------------------------------- full-storage reduction
+// ----------------------------------------------------------------- packed reduction
 template <typename T>
 struct TriShared {
   using C = typename C2<T>::type;
-  C* M;       // n x pitch
-  int pitch;  // odd
+  C* L;       // lower triangle, packed by rows: (i, j <= i) at i(i+1)/2 + j
   C* pv;      // [2][n] products of the last two steps
   C* vec;     // [3][n]: u_k and u_{k-1} (by step parity), w_{k-1}
   C* e;
@@ -174,12 +172,12 @@ struct TriShared {
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
-__host__ __device__ inline int odd_pitch(int n) { return n | 1; }
+__host__ __device__ __forceinline__ int tri(int i) { return i * (i + 1) / 2; }
 
 template <typename T>
 __host__ __device__ inline size_t tri_bytes(int n) {
   using C = typename C2<T>::type;
-  size_t o = align16((size_t)n * odd_pitch(n) * sizeof(C));
+  size_t o = align16((size_t)n * (n + 1) / 2 * sizeof(C));
   o = align16(o + 2 * (size_t)n * sizeof(C));
   o = align16(o + 3 * (size_t)n * sizeof(C));
   o = align16(o + 2 * (size_t)n * sizeof(C));
@@ -192,10 +190,9 @@ template <typename T>
 __device__ inline TriShared<T> tri_layout(unsigned char* base, int n) {
   using C = typename C2<T>::type;
   TriShared<T> s;
-  s.pitch = odd_pitch(n);
   size_t o = 0;
-  s.M = reinterpret_cast<C*>(base + o);
-  o = align16(o + (size_t)n * s.pitch * sizeof(C));
+  s.L = reinterpret_cast<C*>(base + o);
+  o = align16(o + (size_t)n * (n + 1) / 2 * sizeof(C));
   s.pv = reinterpret_cast<C*>(base + o);
   o = align16(o + 2 * (size_t)n * sizeof(C));
   s.vec = reinterpret_cast<C*>(base + o);
@@ -224,20 +221,26 @@ template <typename C> __device__ __forceinline__ void rank2(C& a, C ui, C wj, C 
   a.y -= ui.y * wj.x - ui.x * wj.y + wi.y * uj.x - wi.x * uj.y;
 }
 
-// Householder reduction of the Hermitian M (full storage in s.M) to tridiagonal (s.d, s.e),
-// reflector k stored in column k (rows k+1..n-1) with scalar s.tau[k]. Whole CTA, two
-// barriers per step: warp 0 finishes step k-1 and forms reflector k from column k brought
-// up to date, x_i = A_i + K B_i (A_i, B_i from the same pass as the dot product that gives
-// K = tau/2 u^H p, so one load pass and two warp reductions); then a thread pair per row
-// applies step k-1's update to the row and accumulates (M u_k)_i.
+// Householder reduction of the Hermitian M (lower triangle, packed in s.L) to tridiagonal
+// (s.d, s.e); reflector k stored in column k (rows k+1..n-1) with scalar s.tau[k]. Whole
+// CTA, three barriers per step:
+//   1. warp 0 finishes step k-1 (w = p - K u, K = tau/2 u^H p) and forms reflector k from
+//      column k brought up to date, x_i = A_i + K B_i, with A_i and B_i computed in the same
+//      pass as the dot product (one load pass, two warp reductions);
+//   2. phase 1: step k-1's rank-2 update on the lower triangle of rows >= k+1 and the row
+//      part of (M u_k)_i = sum_{j<=i} M_ij u_j;
+//   3. phase 2: the column part sum_{j>i} conj(M_ji) u_j, then p_k = tau_k M u_k.
+// Rows are handled in mirrored pairs (i, n+k-i) by 4 threads each, which gives every
+// thread the same number of elements in both phases. The packed triangle halves the
+// shared memory of full storage, so twice as many points are in flight per SM.
 template <typename T>
-__device__ void tridiag_full(const TriShared<T>& s, int n) {
+__device__ void tridiag_packed(const TriShared<T>& s, int n) {
   using C = typename C2<T>::type;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  const int P = s.pitch;
-  C* M = s.M;
+  C* L = s.L;
   C* wp = s.vec + 2 * n;  // w_{k-1}
-  const int rr = tid >> 1, h = tid & 1;  // row slot and half of the pair
+  const int pq = tid >> 2, sub = tid & 3;  // row pair, sub-thread of the quad
+  const unsigned quad = 0xFu << (lane & ~3);
   for (int k = 0; k + 2 < n; ++k) {
     C* up = s.vec + ((k + 1) & 1) * n;  // u_{k-1}
     C* uc = s.vec + (k & 1) * n;        // u_k
@@ -255,7 +258,8 @@ __device__ void tridiag_full(const TriShared<T>& s, int n) {
         const int i = k + lane + 32 * t;
         A[t] = B[t] = pp[t] = uu[t] = mk<T>(0, 0);
         if (i < n) {
-          A[t] = M[(size_t)i * P + k];
+          const int base = tri(i);
+          A[t] = L[base + k];
           if (pending) {
             pp[t] = p[i];
             uu[t] = up[i];
@@ -263,11 +267,10 @@ __device__ void tridiag_full(const TriShared<T>& s, int n) {
             // x_i = a_ik - u_i conj(w_k) - w_i conj(u_k) = A_i + K B_i, w = p - K u
             rank2(A[t], uu[t], pk, pp[t], ukk);
             B[t] = mk<T>(2 * (uu[t].x * ukk.x + uu[t].y * ukk.y), 2 * (uu[t].y * ukk.x - uu[t].x * ukk.y));
-            if (i > k) M[(size_t)i * P + k - 1] = uu[t];  // reflector k-1 (rows >= k) kept in column k-1
+            L[base + k - 1] = uu[t];  // reflector k-1 (rows >= k) kept in column k-1
           }
         }
       }
-      if (pending && lane == 0) M[(size_t)k * P + k - 1] = ukk;
       const T K = pending ? T(0.5) * tau_prev * warp_sum(dot) : T(0);
       T xn2 = 0;
 #pragma unroll
@@ -296,43 +299,54 @@ __device__ void tridiag_full(const TriShared<T>& s, int n) {
       if (lane == 0) { s.d[k] = uc[k].x; s.e[k] = ek; s.tau[k] = tau_k; }
     }
     __syncthreads();
-    // ---- row pairs: step k-1's update on rows/cols >= k+1 and p_k = tau_k M u_k
     const bool pending = k > 0 && s.tau[k - 1] != T(0);
     const T tau_k = s.tau[k];
-    const int i = k + 1 + rr;
-    if ((pending || tau_k != T(0)) && i < n) {
-      C* row = M + (size_t)i * P;
-      C upi = mk<T>(0, 0), wpi = mk<T>(0, 0);
-      if (pending) { upi = up[i]; wpi = wp[i]; }
-      C acc0 = mk<T>(0, 0), acc1 = mk<T>(0, 0);
-      int j = k + 1 + h;
-      for (; j + 2 < n; j += 4) {
-        C a0 = row[j], a1 = row[j + 2];
-        if (pending) {
-          rank2(a0, upi, wp[j], wpi, up[j]);
-          rank2(a1, upi, wp[j + 2], wpi, up[j + 2]);
-          row[j] = a0;
-          row[j + 2] = a1;
+    const int m = n - k - 1;         // rows k+1..n-1
+    const int npair = (m + 1) >> 1;  // mirrored pairs (the middle row of an odd m alone)
+    const bool active = (pending || tau_k != T(0)) && pq < npair;
+    const int i1 = k + 1 + pq, i2 = n - 1 - pq;
+    const bool two = i2 != i1;
+    // ---- phase 1: update the lower rows, row part of M u
+    C rs1 = mk<T>(0, 0), rs2 = mk<T>(0, 0);
+    if (active) {
+#pragma unroll 1
+      for (int r = 0; r < 2; ++r) {
+        if (r && !two) break;
+        const int i = r ? i2 : i1;
+        C* row = L + tri(i);
+        C upi = mk<T>(0, 0), wpi = mk<T>(0, 0);
+        if (pending) { upi = up[i]; wpi = wp[i]; }
+        C acc = mk<T>(0, 0);
+        for (int j = k + 1 + sub; j <= i; j += 4) {
+          C a = row[j];
+          if (pending) { rank2(a, upi, wp[j], wpi, up[j]); row[j] = a; }
+          const C u = uc[j];
+          acc.x += a.x * u.x - a.y * u.y;
+          acc.y += a.x * u.y + a.y * u.x;
         }
-        const C u0 = uc[j], u1 = uc[j + 2];
-        acc0.x += a0.x * u0.x - a0.y * u0.y;
-        acc0.y += a0.x * u0.y + a0.y * u0.x;
-        acc1.x += a1.x * u1.x - a1.y * u1.y;
-        acc1.y += a1.x * u1.y + a1.y * u1.x;
+        if (r) rs2 = acc; else rs1 = acc;
       }
-      if (j < n) {
-        C a0 = row[j];
-        if (pending) { rank2(a0, upi, wp[j], wpi, up[j]); row[j] = a0; }
-        const C u0 = uc[j];
-        acc0.x += a0.x * u0.x - a0.y * u0.y;
-        acc0.y += a0.x * u0.y + a0.y * u0.x;
+    }
+    __syncthreads();
+    // ---- phase 2: column part, then p_k
+    if (active && tau_k != T(0)) {
+#pragma unroll 1
+      for (int r = 0; r < 2; ++r) {
+        if (r && !two) break;
+        const int i = r ? i2 : i1;
+        C acc = r ? rs2 : rs1;
+        for (int j = i + 1 + sub; j < n; j += 4) {
+          const C a = L[tri(j) + i];  // M_ji, lower triangle
+          const C u = uc[j];
+          acc.x += a.x * u.x + a.y * u.y;  // conj(M_ji) u_j
+          acc.y += a.x * u.y - a.y * u.x;
+        }
+        acc.x += __shfl_xor_sync(quad, acc.x, 1);
+        acc.y += __shfl_xor_sync(quad, acc.y, 1);
+        acc.x += __shfl_xor_sync(quad, acc.x, 2);
+        acc.y += __shfl_xor_sync(quad, acc.y, 2);
+        if (sub == 0) s.pv[(k & 1) * n + i] = mk<T>(tau_k * acc.x, tau_k * acc.y);
       }
-      acc0 = cadd(acc0, acc1);
-      // the pair (lanes 2r, 2r+1) is active together: i depends only on tid >> 1
-      const unsigned pair = 3u << (lane & ~1);
-      acc0.x += __shfl_xor_sync(pair, acc0.x, 1);
-      acc0.y += __shfl_xor_sync(pair, acc0.y, 1);
-      if (h == 0 && tau_k != T(0)) s.pv[(k & 1) * n + i] = mk<T>(tau_k * acc0.x, tau_k * acc0.y);
     }
     __syncthreads();
   }
@@ -353,15 +367,15 @@ __device__ void tridiag_full(const TriShared<T>& s, int n) {
       __syncwarp();
       if (lane < 3) {
         const int i = (lane == 0) ? n - 2 : n - 1, j = (lane == 2) ? n - 1 : n - 2;
-        rank2(M[(size_t)i * P + j], up[i], wp[j], wp[i], up[j]);
+        rank2(L[tri(i) + j], up[i], wp[j], wp[i], up[j]);
       }
-      for (int i = n - 2 + lane; i < n; i += 32) M[(size_t)i * P + n - 3] = up[i];
+      for (int i = n - 2 + lane; i < n; i += 32) L[tri(i) + n - 3] = up[i];
       __syncwarp();
     }
     if (lane == 0) {
-      s.d[n - 2] = M[(size_t)(n - 2) * P + n - 2].x;
-      s.d[n - 1] = M[(size_t)(n - 1) * P + n - 1].x;
-      s.e[n - 2] = M[(size_t)(n - 1) * P + n - 2];
+      s.d[n - 2] = L[tri(n - 2) + n - 2].x;
+      s.d[n - 1] = L[tri(n - 1) + n - 1].x;
+      s.e[n - 2] = L[tri(n - 1) + n - 2];
     }
   }
   __syncthreads();
@@ -439,38 +453,40 @@ __global__ void __launch_bounds__(kThreads, 1) inverse_kernel(const float2* __re
 
 // ----------------------------------------------------------------- kernel 2: reduction
 template <typename T>
-__global__ void __launch_bounds__(kThreads) reduce_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 2) reduce_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
                                                          unsigned char* __restrict__ ws) {
-  using C = typename C2<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const TriShared<T> s = tri_layout<T>(smem_raw, n);
   const int tid = threadIdx.x, nt = blockDim.x;
   const int64_t npairs = (int64_t)n * (n - 1) / 2;
-  const int P = s.pitch;
+  const int np = n * (n + 1) / 2;
   for (int64_t pt = blockIdx.x; pt < n_pc; pt += gridDim.x) {
     const float2* c = coh + pt * npairs;
     PointPtr<T> w(ws, pt, n);
-    for (int e = tid; e < n * n; e += nt) {  // M = inv(|Gamma|) o Gamma, full
-      const int i = e / n, j = e - i * n;
-      const int hi = max(i, j), lo = min(i, j);
+    // M = inv(|Gamma|) o Gamma, lower triangle packed like inv(|Gamma|) itself
+    int i = 0;
+    while (tri(i + 1) <= tid) ++i;
+    for (int q = tid; q < np; q += nt) {
+      while (tri(i + 1) <= q) ++i;
+      const int j = q - tri(i);
       T gx = 1, gy = 0;
       if (i != j) {
-        const float2 g = c[triu_index(lo, hi, n)];
+        const float2 g = c[triu_index(j, i, n)];
         gx = g.x;
-        gy = i < j ? g.y : -g.y;
+        gy = -g.y;  // Gamma_ij = conj(Gamma_ji) for i > j
       }
-      const T sc = w.ainv[(int64_t)hi * (hi + 1) / 2 + lo];
-      s.M[(size_t)i * P + j] = mk<T>(sc * gx, sc * gy);
+      const T sc = w.ainv[q];
+      s.L[q] = mk<T>(sc * gx, sc * gy);
     }
     __syncthreads();
-    tridiag_full<T>(s, n);
-    for (int i = tid; i < n; i += nt) {
-      w.d[i] = s.d[i];
-      w.tau[i] = (i + 2 < n) ? s.tau[i] : T(0);
-      if (i + 1 < n) w.e[i] = s.e[i];
+    tridiag_packed<T>(s, n);
+    for (int k = tid; k < n; k += nt) {
+      w.d[k] = s.d[k];
+      w.tau[k] = (k + 2 < n) ? s.tau[k] : T(0);
+      if (k + 1 < n) w.e[k] = s.e[k];
     }
     for (int k = 0; k + 2 < n; ++k)  // reflector k: column k, rows k+1..n-1
-      for (int i = tid; i < n - k - 1; i += nt) w.refl[refl_off(k, n) + i] = s.M[(size_t)(k + 1 + i) * P + k];
+      for (int r = tid; r < n - k - 1; r += nt) w.refl[refl_off(k, n) + r] = s.L[tri(k + 1 + r) + k];
     __syncthreads();
   }
 }
