@@ -113,6 +113,89 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
+DTYPE = {"fp32": "f32", "bf16": "bf16 Gram, f32 EMI", "bf16x3": "bf16x3 Gram, f32 EMI", "fp64": "f64"}
+
+# DRAM bytes per DS point of one mr_emi call (inverse + reduce + tail kernels), from the
+# ncu capture of the 2000 x 2000 x 100 scene's EMI sub-batch (N = 100)
+EMI_TRAFFIC_PER_POINT = {100: None}
+
+
+def fp32_simt_peak(dev) -> float:
+    """FP32 FMA-pipe reference rate in TFLOP/s: cuBLAS SGEMM 8192^3 with TF32 off, best of 5."""
+    import torch  # noqa: PLC0415
+
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        a = torch.randn(8192, 8192, device=dev)
+        b = torch.randn(8192, 8192, device=dev)
+        c = a @ b
+        best = 0.0
+        for _ in range(5):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b, out=c)
+            e1.record()
+            e1.synchronize()
+            best = max(best, 2 * 8192 ** 3 / (e0.elapsed_time(e1) / 1e3) / 1e12)
+        del a, b, c
+        return best
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = old
+
+
+def stage_rooflines(cfg, stage: dict, n_ds: int, res, peaks: dict, fp32: float, chain, precision: str) -> dict:
+    """Achieved rate of every stage against the bound that limits it.
+
+    Algorithmic work per unit (unit = pixel for the raster stages, DS point for the rest):
+      ks_select   4N + W + 4 bytes per pixel (rmli in, mask and count out), W(2N-1) merge steps
+      coherence   8 S Q + 3 S N flops per DS point (S = its SHP count, Q = N(N-1)/2)
+      emi_tcoh    2.7 N^3 + 80 N^2 flops per DS point (Cholesky + inverse of |Gamma|, complex
+                  factorisation of M, inverse-iteration solves)
+    """
+    n = cfg.nimages
+    npix = cfg.nlines * cfg.width
+    q = n * (n - 1) // 2
+    hbm = peaks.get("hbm_gbs")
+    out = {}
+    if stage.get("ks_select"):
+        ms = stage["ks_select"] + stage.get("intensity", 0.0)
+        byts = npix * (4 * n + cfg.az_win * cfg.r_win + 4) + npix * n * 12
+        gbs = byts / (ms / 1e3) / 1e9
+        out["ks_select"] = {"kernel": "intensity_kernel + sort_keys_kernel + ks_merge_kernel", "bound": "hbm",
+                            "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "traffic": None,
+                            "ms": ms, "merge_steps_per_s": npix * cfg.az_win * cfg.r_win * (2 * n - 1) / (ms / 1e3),
+                            "peak_source": peaks["source"]}
+    if stage.get("coherence") and n_ds:
+        ms = stage["coherence"]
+        idx = res.idx.long()
+        s = res.shp_num[idx[:, 0], idx[:, 1]].double()
+        flops = float((8 * s * q + 3 * s * n).sum().item())
+        tf = flops / (ms / 1e3) / 1e12
+        tc = precision in ("bf16", "bf16x3")
+        peak = peaks.get("bf16_tflops") if tc else fp32
+        out["coherence"] = {"kernel": "gram_tc_kernel" if tc else "gram_kernel", "bound": "tensor" if tc else
+                            "fp32-simt", "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
+                            "traffic": None, "ms": ms,
+                            "peak_source": peaks["source"] + " bf16" if tc else "cuBLAS SGEMM in this run"}
+    if stage.get("emi_tcoh") and n_ds:
+        ms = stage["emi_tcoh"]
+        calls = -(-n_ds // chain.batch)
+        flops = n_ds * (2.7 * n ** 3 + 80 * n ** 2)
+        tf = flops / (ms / 1e3) / 1e12
+        tpp = EMI_TRAFFIC_PER_POINT.get(n)
+        f64 = precision == "fp64" or n > 128
+        peak = fp32 / 2 if f64 else fp32  # the FP64 pipe of B200 runs at half the FP32 rate
+        out["emi_tcoh"] = {"kernel": "mr_emi: inverse_kernel + reduce_kernel + tail_kernel", "bound":
+                           "fp64-simt" if f64 else "fp32-simt",
+                           "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
+                           "traffic": tpp * n_ds / calls if tpp else None, "ms": ms,
+                           "launches": calls, "peak_source": "cuBLAS SGEMM in this run (FP32, TF32 off)",
+                           "executed_flops_per_point": 2 * n ** 3 + 16 * n ** 3 / 3}
+    return out
+
+
 # ----------------------------------------------------------------------------- CPU leg
 def cpu_threads() -> int:
     """Host threads for the CPU legs: all cores this process may use, capped at 64."""
@@ -209,7 +292,7 @@ def main():
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/c64 (f64 accumulate)",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": workload,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
                              "sample": f"{side}x{side} crop of the scene model per step ({int(np.mean(nds))} DS "
@@ -261,11 +344,14 @@ def main():
     barrier()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
+    lib = _lib.load()
+    launches0 = lib.mr_kernel_launches()
     t0.record()
     for _ in range(args.steps):
         res = chain.run(rslc)
     t1.record()
     barrier()
+    launches = int(lib.mr_kernel_launches() - launches0)
     clk = clocks.stop()
     ms = t0.elapsed_time(t1) / args.steps
     log(f"timed: {ms:.1f} ms per step")
@@ -320,35 +406,15 @@ def main():
                "h2d_bytes_per_step": int(rslc.numel() * 8), "d2h_bytes_per_step": int(d2h + 8),
                "path": "moraine_b200.chain.DsChain.run on a pinned host stack, results copied back"}
 
-    # roofline of the dominant stage (filled by kernel-level timing in the stage split)
+    # rooflines: every stage against its bound; the headline is the dominant stage
     peaks = measured_peaks()
-    dom = max(stage, key=stage.get) if stage else None
-    roofline = None
-    if dom:
-        N = cfg.nimages
-        dom_ms = stage[dom]
-        if dom == "emi_tcoh":
-            flops = n_ds * (2.7 * N ** 3 + 80 * N ** 2)
-            achieved = flops / (dom_ms / 1e3) / 1e12
-            roofline = {"kernel": "emi_kernel", "bound": "fp64-simt", "achieved": achieved, "unit": "TFLOP/s",
-                        "peak": None, "frac": None, "traffic": None,
-                        "note": "EMI runs on FP64 CUDA cores; algorithmic flops 2.7N^3+80N^2 per DS point"}
-        elif dom == "coherence":
-            q = N * (N - 1) // 2
-            mean_s = float(res.shp_num.float().mean().item())
-            flops = n_ds * (8 * mean_s * q + 3 * mean_s * N)
-            achieved = flops / (dom_ms / 1e3) / 1e12
-            roofline = {"kernel": "gram_kernel", "bound": "tensor", "achieved": achieved, "unit": "TFLOP/s",
-                        "peak": peaks.get("bf16_tflops"), "frac": achieved / peaks.get("bf16_tflops"),
-                        "traffic": None}
-        else:
-            npix = cfg.nlines * cfg.width
-            byts = npix * (4 * cfg.nimages + cfg.az_win * cfg.r_win + 4)
-            achieved = byts / (dom_ms / 1e3) / 1e9
-            roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "unit": "GB/s",
-                        "peak": peaks.get("hbm_gbs"), "frac": achieved / peaks.get("hbm_gbs"), "traffic": None}
-        roofline["peak_source"] = peaks["source"]
-
+    fp32 = fp32_simt_peak(dev)
+    log(f"FP32 SIMT reference rate: {fp32:.1f} TFLOP/s (cuBLAS SGEMM, TF32 off)")
+    stage_roof = stage_rooflines(cfg, stage, n_ds, res, peaks, fp32, chain, args.precision)
+    dom = max(stage_roof, key=lambda k: stage_roof[k]["ms"]) if stage_roof else None
+    roofline = dict(stage_roof[dom]) if dom else None
+    if roofline:
+        roofline["stage"] = dom
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = cpu_threads()
@@ -365,13 +431,13 @@ def main():
         log("cpu baseline done")
 
     if rank == 0:
-        launches_per_step = 4 + 2 * max(1, -(-n_ds // chain.batch))
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32/c64 Gram, f64 EMI, u32 KS keys", "data": "synthetic",
+            "vs_baseline": None, "dtype": DTYPE[args.precision], "data": "synthetic",
             "config": workload, "n_ds_per_gpu": n_ds, "stage_ms": stage, "roofline": roofline,
-            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches_per_step * args.steps,
+            "stage_roofline": stage_roof,
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
         }))
     if world > 1:
         dist.destroy_process_group()

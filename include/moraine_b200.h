@@ -59,6 +59,10 @@ enum {
 #define MR_MAX_WINDOW 4096 /* az_win * r_win */
 
 const char* mr_last_error(void);
+
+/* Number of kernels the library has launched in this process (all devices, all
+ * streams), for accounting by benchmarks and tests. No reference counterpart. */
+uint64_t mr_kernel_launches(void);
 int mr_abi_version(void);
 
 /* ---------------------------------------------------------------- intensity prologue

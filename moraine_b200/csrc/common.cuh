@@ -14,7 +14,12 @@ namespace mr {
 void set_error(const char* fmt, ...);
 int fail(int code, const char* fmt, ...);
 
-inline int check_launch(const char* what) {
+// Kernel launches made by the library since the process started (mr_kernel_launches()).
+void note_launches(int k);
+
+// Status of the launches just made; counts them.
+inline int check_launch(const char* what, int launches = 1) {
+  note_launches(launches);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(MR_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
   return MR_OK;

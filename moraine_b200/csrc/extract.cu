@@ -145,7 +145,7 @@ extern "C" int mr_ds_extract(const int32_t* shp_num, const uint8_t* is_shp, int 
   scan_kernel<<<1, 1024, 0, s>>>(counts, nblocks, n_ds);
   scatter_kernel<<<(unsigned)nblocks, kThreads, 0, s>>>(shp_num, is_shp, npix, width, win, min_shp,
                                                         counts, idx, pc_is_shp, max_ds);
-  return check_launch("ds_extract");
+  return check_launch("ds_extract", 3);
 }
 
 // ------------------------------------------------------------------------------------
@@ -217,5 +217,5 @@ extern "C" int mr_ds_extract_noalloc(const int32_t* shp_num, const uint8_t* is_s
   scan_kernel<<<1, 1024, 0, s>>>(counts, nblocks, n_ds);
   scatter_kernel<<<(unsigned)nblocks, kThreads, 0, s>>>(shp_num, is_shp, npix, width, win, min_shp, counts, idx,
                                                         pc_is_shp, max_ds);
-  return check_launch("ds_extract_noalloc");
+  return check_launch("ds_extract_noalloc", 3);
 }

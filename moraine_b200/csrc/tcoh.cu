@@ -132,5 +132,5 @@ extern "C" int mr_uncompress_coh(const mr_complex64* coh, int64_t n, int nimages
   if (n_pairs > 0)
     uncompress_scatter_kernel<<<grid_for(n * n_pairs, 256), 256, 0, s>>>(reinterpret_cast<const float2*>(coh), n,
                                                                         nimages, image_pairs, n_pairs, o);
-  return check_launch("uncompress_coh");
+  return check_launch("uncompress_coh", n_pairs > 0 ? 2 : 1);
 }

@@ -1,4 +1,5 @@
 // Error reporting, version and device queries of the moraine_b200 C ABI.
+#include <atomic>
 #include <cstdarg>
 #include <mutex>
 
@@ -38,5 +39,12 @@ int sm_count() {
 }  // namespace mr
 
 extern "C" const char* mr_last_error(void) { return mr::g_last_error; }
+
+namespace mr {
+static std::atomic<uint64_t> g_launches{0};
+void note_launches(int k) { g_launches.fetch_add((uint64_t)k, std::memory_order_relaxed); }
+}  // namespace mr
+
+extern "C" uint64_t mr_kernel_launches(void) { return mr::g_launches.load(std::memory_order_relaxed); }
 
 extern "C" int mr_abi_version(void) { return 1; }
