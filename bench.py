@@ -46,6 +46,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=160, help="side of the crop timed on the host")
+    ap.add_argument("--serve-requests", type=int, default=16, help="tiles in the serving episode (0: none)")
+    ap.add_argument("--serve-rate", type=float, default=8.0, help="Poisson arrival rate of tiles per second")
+    ap.add_argument("--serve-slots", type=int, default=4, help="tiles in flight at once")
+    ap.add_argument("--serve-full", action="store_true",
+                    help="full serving workload: tiles up to 2048^2 and nimage up to 150 (default: up to 1024^2, 100)")
     return ap.parse_args()
 
 
@@ -194,6 +199,54 @@ def stage_rooflines(cfg, stage: dict, n_ds: int, res, peaks: dict, fp32: float, 
                            "launches": calls, "peak_source": "cuBLAS SGEMM in this run (FP32, TF32 off)",
                            "executed_flops_per_point": 2 * n ** 3 + 16 * n ** 3 / 3}
     return out
+
+
+# ----------------------------------------------------------------------------- serving
+def serving_episode(dev, args) -> dict:
+    """p50/p99 tile latency of a Poisson stream of tiles through the request loop.
+
+    The stream is served twice after a warm-up pass: with ``--serve-slots`` tiles in flight
+    under a 150 GB admission budget and arrivals in real time (latency), and one tile at a
+    time with every tile queued at once (the plain chain's throughput on the same tiles).
+    """
+    import torch  # noqa: PLC0415
+
+    from moraine_b200.serve import DsServer, TileRequest, latency_summary  # noqa: PLC0415
+    from moraine_b200.synth import SERVING_NIMAGES, SERVING_SIZES, make_stack, serving_stream  # noqa: PLC0415
+
+    sizes = SERVING_SIZES if args.serve_full else SERVING_SIZES[:3]
+    nimg = SERVING_NIMAGES if args.serve_full else SERVING_NIMAGES[:3]
+    specs = serving_stream(args.serve_requests, args.serve_rate, sizes=sizes, nimages=nimg)
+    stacks = {}
+    for sp in specs:  # drawn on the device, served from pinned host memory
+        stacks[sp.request_id] = make_stack(sp.scene(), device=dev).cpu().pin_memory()
+    torch.cuda.synchronize()
+
+    def run(slots: int, realtime: bool) -> list:
+        srv = DsServer(hbm_budget=150e9, slots=slots, device=dev)
+        t0 = time.perf_counter()
+        futs = []
+        for sp in specs:
+            at = t0 + sp.arrival_s if realtime else t0
+            while realtime and time.perf_counter() < at:
+                time.sleep(min(0.002, max(0.0, at - time.perf_counter())))
+            futs.append(srv.submit(TileRequest(rslc=stacks[sp.request_id], az_half_win=sp.az_half_win,
+                                               r_half_win=sp.r_half_win, request_id=sp.request_id, arrival=at)))
+        out = [f.result() for f in futs]
+        srv.close()
+        return out
+
+    run(args.serve_slots, False)  # warm-up: kernels, plans, allocator
+    served = latency_summary(run(args.serve_slots, True))
+    plain = latency_summary(run(1, False))
+    return {"p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"], "mean_ms": served["mean_ms"],
+            "max_ms": served["max_ms"], "requests": served["requests"], "n_ds": served["n_ds"],
+            "ds_pixels_per_s": served["ds_pixels_per_s"], "span_s": served["span_s"],
+            "one_at_a_time_ds_pixels_per_s": plain["ds_pixels_per_s"], "slots": args.serve_slots,
+            "hbm_budget_gb": 150, "rate_per_s": args.serve_rate,
+            "workload": f"{len(specs)} Poisson tiles, sizes {list(sizes)}^2, nimage {list(nimg)}, windows "
+                        f"11x11/11x21/15x31, small-scene generator with one seed per tile, from pinned host "
+                        f"memory; latency = arrival to results in host memory"}
 
 
 # ----------------------------------------------------------------------------- CPU leg
@@ -415,6 +468,12 @@ def main():
     roofline = dict(stage_roof[dom]) if dom else None
     if roofline:
         roofline["stage"] = dom
+    latency = None
+    if args.serve_requests > 0:
+        log(f"serving episode: {args.serve_requests} tiles")
+        latency = serving_episode(dev, args)
+        log(f"serving: p50 {latency['p50_ms']:.1f} ms, p99 {latency['p99_ms']:.1f} ms")
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = cpu_threads()
@@ -437,7 +496,7 @@ def main():
             "vs_baseline": None, "dtype": DTYPE[args.precision], "data": "synthetic",
             "config": workload, "n_ds_per_gpu": n_ds, "stage_ms": stage, "roofline": roofline,
             "stage_roofline": stage_roof,
-            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+            "cpu_baseline": cpu, "e2e": e2e, "latency": latency, "clocks": clk, "gpu_launches": launches,
         }))
     if world > 1:
         dist.destroy_process_group()

@@ -49,9 +49,7 @@ class DsChain:
         self.timing = timing
         self.npairs = nimages * (nimages - 1) // 2
         npix = nlines * width
-        if batch is None:
-            batch = max(1024, min(npix, (8 << 30) // (8 * self.npairs)))  # <= 8 GiB coherence per batch
-        self.batch = int(batch)
+        self.batch = int(self.default_batch(npix, nimages) if batch is None else batch)
         lib = _lib.load()
         d = self.device
         self.rmli = torch.empty((nlines, width, nimages), dtype=torch.float32, device=d)
@@ -66,6 +64,25 @@ class DsChain:
         self.ph = torch.empty((npix, nimages), dtype=torch.complex64, device=d)
         self.quality = torch.empty((npix,), dtype=torch.float32, device=d)
         self.t_coh = torch.empty((npix,), dtype=torch.float32, device=d)
+
+    @staticmethod
+    def default_batch(npix: int, nimages: int) -> int:
+        """DS points per coherence + EMI batch: at most 8 GiB of coherence."""
+        npairs = nimages * (nimages - 1) // 2
+        return max(1024, min(npix, (8 << 30) // (8 * npairs)))
+
+    @staticmethod
+    def footprint(nlines: int, width: int, nimages: int, az_half_win: int, r_half_win: int,
+                  batch: int | None = None) -> int:
+        """Device bytes the buffers of a plan of this shape occupy."""
+        lib = _lib.load()
+        npix = nlines * width
+        win = (2 * az_half_win + 1) * (2 * r_half_win + 1)
+        npairs = nimages * (nimages - 1) // 2
+        batch = DsChain.default_batch(npix, nimages) if batch is None else batch
+        return int(npix * nimages * 4 + lib.mr_ks_workspace_bytes(nlines, width, nimages) + npix * win + npix * 4
+                   + lib.mr_ds_extract_workspace_bytes(npix) + npix * 8 + 8 + batch * npairs * 8
+                   + lib.mr_emi_workspace_bytes(batch, nimages) + npix * nimages * 8 + npix * 8)
 
     def run(self, rslc: torch.Tensor) -> ChainResult:
         nlines, width, n = self.shape

@@ -23,6 +23,7 @@ from __future__ import annotations
 import math
 from dataclasses import dataclass, replace
 
+import numpy as np
 import torch
 
 WAVELENGTH_MM = 56.0  # C-band, 5.6 cm
@@ -171,6 +172,45 @@ def make_stack(cfg: SceneConfig, device="cpu", return_truth: bool = False):
         return rslc, {"labels": labels, "ps_mask": ps_mask.reshape(H, W), "phase": phase,
                       "intensity": intensity, "velocity": vel}
     return rslc
+
+
+@dataclass(frozen=True)
+class TileSpec:
+    """One request of a serving stream: a tile drawn from the small-scene generator."""
+    request_id: int
+    size: int
+    nimages: int
+    az_half_win: int
+    r_half_win: int
+    seed: int
+    arrival_s: float
+
+    def scene(self) -> SceneConfig:
+        # the small-scene model (12 patches per 200 x 200 pixels) at this tile's size
+        patches = max(4, round(12 * self.size * self.size / (200 * 200)))
+        return CONFIGS["c0"].scaled(nlines=self.size, width=self.size, nimages=self.nimages,
+                                    az_half_win=self.az_half_win, r_half_win=self.r_half_win,
+                                    n_patches=patches, seed=self.seed)
+
+
+# Serving workload: tile sizes, nimage and windows drawn uniformly, Poisson arrivals.
+SERVING_SIZES = (256, 512, 1024, 2048)
+SERVING_NIMAGES = (20, 50, 100, 150)
+SERVING_WINDOWS = ((5, 5), (5, 10), (7, 15))  # 11x11, 11x21, 15x31
+
+
+def serving_stream(n_requests: int, rate_per_s: float, seed: int = 4, sizes=SERVING_SIZES,
+                   nimages=SERVING_NIMAGES, windows=SERVING_WINDOWS) -> list[TileSpec]:
+    """A Poisson stream of ``n_requests`` tile requests, each with its own generator seed."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_per_s, size=n_requests))
+    t -= t[0]
+    out = []
+    for i in range(n_requests):
+        azh, rh = windows[rng.integers(len(windows))]
+        out.append(TileSpec(i, int(sizes[rng.integers(len(sizes))]), int(nimages[rng.integers(len(nimages))]),
+                            int(azh), int(rh), int(seed * 100000 + i), float(t[i])))
+    return out
 
 
 def rmli_of(rslc: torch.Tensor) -> torch.Tensor:
