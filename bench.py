@@ -42,7 +42,10 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", default="c2")
     ap.add_argument("--size", type=int, default=0, help="override nlines = width (smaller runs)")
-    ap.add_argument("--precision", default="fp32")
+    ap.add_argument("--precision", default="fp64", help="coherence Gram arithmetic: fp64, fp32, bf16x3, bf16")
+    ap.add_argument("--emi-precision", default=None, help="EMI arithmetic: fp64, fp32 or mixed (default: fp64 "
+                                                          "with an fp64 Gram, else fp32)")
+    ap.add_argument("--no-variants", action="store_true", help="skip the precision variants")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=160, help="side of the crop timed on the host")
@@ -179,25 +182,75 @@ def stage_rooflines(cfg, stage: dict, n_ds: int, res, peaks: dict, fp32: float, 
         flops = float((8 * s * q + 3 * s * n).sum().item())
         tf = flops / (ms / 1e3) / 1e12
         tc = precision in ("bf16", "bf16x3")
-        peak = peaks.get("bf16_tflops") if tc else fp32
+        g64 = precision == "fp64"
+        peak = peaks.get("bf16_tflops") if tc else (fp32 / 2 if g64 else fp32)
         out["coherence"] = {"kernel": "gram_tc_kernel" if tc else "gram_kernel", "bound": "tensor" if tc else
-                            "fp32-simt", "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
-                            "traffic": None, "ms": ms,
-                            "peak_source": peaks["source"] + " bf16" if tc else "cuBLAS SGEMM in this run"}
+                            ("fp64-simt" if g64 else "fp32-simt"), "achieved": tf, "peak": peak, "unit": "TFLOP/s",
+                            "frac": tf / peak, "traffic": None, "ms": ms,
+                            "peak_source": peaks["source"] + " bf16" if tc else
+                            "cuBLAS SGEMM in this run (FP32, TF32 off)" + (", halved for the FP64 pipe" if g64 else "")}
     if stage.get("emi_tcoh") and n_ds:
         ms = stage["emi_tcoh"]
         calls = -(-n_ds // chain.batch)
         flops = n_ds * (2.7 * n ** 3 + 80 * n ** 2)
         tf = flops / (ms / 1e3) / 1e12
         tpp = EMI_TRAFFIC_PER_POINT.get(n)
-        f64 = precision == "fp64" or n > 128
+        f64 = chain.emi_precision == "fp64" or n > 128
         peak = fp32 / 2 if f64 else fp32  # the FP64 pipe of B200 runs at half the FP32 rate
         out["emi_tcoh"] = {"kernel": "mr_emi: inverse_kernel + reduce_kernel + tail_kernel", "bound":
                            "fp64-simt" if f64 else "fp32-simt",
                            "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
                            "traffic": tpp * n_ds / calls if tpp else None, "ms": ms,
-                           "launches": calls, "peak_source": "cuBLAS SGEMM in this run (FP32, TF32 off)",
+                           "launches": calls, "peak_source": "cuBLAS SGEMM in this run (FP32, TF32 off)"
+                           + (", halved for the FP64 pipe" if f64 else ""),
                            "executed_flops_per_point": 2 * n ** 3 + 16 * n ** 3 / 3}
+    return out
+
+
+# ----------------------------------------------------------------------------- precision
+def precision_variants(cfg, rslc, ref, dev) -> dict:
+    """Time and accuracy of lower-precision chains against the FP64 chain on the same stack.
+
+    For each variant: DS pixels/s of one pass (after a warm-up pass), the fraction of DS
+    points whose phase history is within 1 mrad of the FP64 chain's, the largest and
+    99th-percentile phase error in rad, the largest temporal-coherence error, the share of
+    points routed to FP64 (mixed EMI), and the largest coherence error over the first
+    20,000 DS points (the Gram alone, against its FP64 accumulation).
+    """
+    import torch  # noqa: PLC0415
+
+    import moraine_b200 as mb  # noqa: PLC0415
+    from moraine_b200.chain import DsChain  # noqa: PLC0415
+
+    ref_ph, ref_t = ref.ph.clone(), ref.t_coh.clone()
+    idx = ref.idx[:20000]
+    pc = ref.is_shp[idx[:, 0].long(), idx[:, 1].long()].view(torch.bool)
+    coh64 = mb.emperical_co_pc(rslc, idx, pc, precision="fp64")
+    out = {}
+    for gram, emi in (("fp32", "fp32"), ("fp64", "mixed"), ("fp32", "mixed")):
+        ch = DsChain(cfg.nlines, cfg.width, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp,
+                     precision=gram, emi_precision=emi, device=dev)
+        ch.run(rslc)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = ch.run(rslc)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        err = (r.ph * ref_ph.conj()).angle().abs().amax(-1)
+        fin = torch.isfinite(err)
+        e = err[fin].sort().values
+        co = mb.emperical_co_pc(rslc, idx, pc, precision=gram)
+        out[f"gram {gram}, emi {emi}"] = {
+            "ds_pixels_per_s": r.n_ds / (ms / 1e3), "ms_per_step": ms,
+            "frac_within_1mrad": float((err <= 1e-3).float().mean()),
+            "phase_err_max_rad": float(e[-1]) if e.numel() else None,
+            "phase_err_p99_rad": float(e[int(0.99 * (e.numel() - 1))]) if e.numel() else None,
+            "t_coh_err_max": float((r.t_coh - ref_t).abs()[fin].max()) if e.numel() else None,
+            "coh_err_max_abs": float((co - coh64).abs().max()),
+            "routed_to_fp64": float((r.route != 0).float().mean()) if r.route is not None else 0.0,
+            "nan_points": int((~fin).sum())}
+        del ch, r
     return out
 
 
@@ -231,7 +284,9 @@ def serving_episode(dev, args) -> dict:
             while realtime and time.perf_counter() < at:
                 time.sleep(min(0.002, max(0.0, at - time.perf_counter())))
             futs.append(srv.submit(TileRequest(rslc=stacks[sp.request_id], az_half_win=sp.az_half_win,
-                                               r_half_win=sp.r_half_win, request_id=sp.request_id, arrival=at)))
+                                               r_half_win=sp.r_half_win, precision=args.precision,
+                                               emi_precision=args.emi_precision, request_id=sp.request_id,
+                                               arrival=at)))
         out = [f.result() for f in futs]
         srv.close()
         return out
@@ -374,7 +429,8 @@ def main():
     torch.cuda.synchronize()
     log("stack ready")
     chain = DsChain(cfg.nlines, cfg.width, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp,
-                    precision=args.precision, device=dev)
+                    precision=args.precision, emi_precision=args.emi_precision, device=dev)
+    workload["emi_precision"] = chain.emi_precision
 
     def barrier():
         if world > 1:
@@ -459,6 +515,11 @@ def main():
                "h2d_bytes_per_step": int(rslc.numel() * 8), "d2h_bytes_per_step": int(d2h + 8),
                "path": "moraine_b200.chain.DsChain.run on a pinned host stack, results copied back"}
 
+    # precision variants on the same stack, against the headline's FP64 chain
+    variants = None
+    if not args.no_variants and rank == 0 and args.precision == "fp64" and chain.emi_precision == "fp64":
+        variants = precision_variants(cfg, rslc, res, dev)
+
     # rooflines: every stage against its bound; the headline is the dominant stage
     peaks = measured_peaks()
     fp32 = fp32_simt_peak(dev)
@@ -495,7 +556,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": DTYPE[args.precision], "data": "synthetic",
             "config": workload, "n_ds_per_gpu": n_ds, "stage_ms": stage, "roofline": roofline,
-            "stage_roofline": stage_roof,
+            "stage_roofline": stage_roof, "precision_variants": variants,
             "cpu_baseline": cpu, "e2e": e2e, "latency": latency, "clocks": clk, "gpu_launches": launches,
         }))
     if world > 1:

@@ -52,7 +52,12 @@ enum {
   MR_PREC_BF16 = 1,   /* BF16 tensor-core Gram, FP32 accumulate */
   MR_PREC_BF16X3 = 2, /* BF16 hi/lo split tensor-core Gram (3 products) */
   MR_PREC_FP64 = 3,   /* FP64 Gram; FP64 EMI */
+  MR_PREC_MIXED = 4,  /* EMI only: FP32, with points whose cond_1(|Gamma|) estimate exceeds
+                         the threshold (or that are singular in FP32) redone in FP64 */
 };
+
+/* Condition threshold of MR_PREC_MIXED in mr_emi. */
+#define MR_EMI_COND_MAX 1.0e4
 
 /* Limits of this build. */
 #define MR_MAX_NIMAGES 512
@@ -152,15 +157,29 @@ int mr_uncompress_coh(const mr_complex64* coh, int64_t n, int nimages,
  * Replaces moraine.pl.emi (moraine/pl.py:68-77; GPU :19-42, CPU :46-65): for every
  * point, M = inv(|Gamma|) o Gamma from the full-triangle compressed coherence, its
  * algebraically smallest eigenpair (lambda, v), ph = v conj(v[ref]) / |v conj(v[ref])|,
- * emi_quality = lambda. inv(|Gamma|) by pivoted Gauss-Jordan in FP64; eigenpair by
- * Householder tridiagonalisation, Sturm bisection and inverse iteration in the arithmetic
- * given by precision (MR_PREC_FP32 or MR_PREC_FP64; FP64 throughout when nimages > 128).
- * t_coh (may be NULL) receives moraine.pl.ds_temp_coh of the result (moraine/pl.py:126)
- * computed in the same pass. workspace: >= mr_emi_workspace_bytes(). */
+ * emi_quality = lambda. inv(|Gamma|) by Gauss-Jordan with partial pivoting; eigenpair by
+ * Householder tridiagonalisation, Sturm multisection and inverse iteration; all in the
+ * arithmetic given by precision: MR_PREC_FP32, MR_PREC_FP64, or MR_PREC_MIXED (FP32, and
+ * FP64 for the points whose cond_1(|Gamma|) estimate exceeds MR_EMI_COND_MAX); FP64
+ * throughout when nimages > 128. t_coh (may be NULL) receives moraine.pl.ds_temp_coh of
+ * the result (moraine/pl.py:126) computed in the same pass. Points whose |Gamma| is
+ * singular at the arithmetic used get NaN (the reference's inv raises on them).
+ * workspace: >= mr_emi_workspace_bytes() (the same for every precision). */
 size_t mr_emi_workspace_bytes(int64_t n_pc, int nimages);
 int mr_emi(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, int precision,
            mr_complex64* ph, float* emi_quality, float* t_coh, void* workspace,
            size_t workspace_bytes, mr_stream_t stream);
+
+/* mr_emi with MR_PREC_MIXED and a caller-chosen threshold cond_max (> 0). Every point is
+ * computed in FP32, cond_1(|Gamma|) = |A|_1 |inv(A)|_1 (A = |Gamma|) is evaluated from the
+ * FP32 inverse, and the points above cond_max or singular in FP32 are recomputed in FP64.
+ * route (may be NULL, n_pc bytes) receives per point 0 = FP32, 1 = FP64 (condition),
+ * 2 = FP64 (singular in FP32); 1 for every point when nimages > 128 (FP64 throughout).
+ * Same computation as moraine.pl.emi (moraine/pl.py:68-77); the routing has no reference
+ * counterpart (the reference runs complex64 LAPACK / cuSOLVER throughout). */
+int mr_emi_routed(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, double cond_max,
+                  mr_complex64* ph, float* emi_quality, float* t_coh, uint8_t* route,
+                  void* workspace, size_t workspace_bytes, mr_stream_t stream);
 
 /* ---------------------------------------------------------------- temporal coherence
  * Replaces moraine.pl.ds_temp_coh (moraine/pl.py:126-145; kernel :104-123):

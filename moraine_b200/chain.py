@@ -28,6 +28,7 @@ class ChainResult:
     shp_num: torch.Tensor      # (nlines, width) int32
     is_shp: torch.Tensor       # (nlines, width, az_win, r_win) uint8
     stage_ms: dict = field(default_factory=dict)
+    route: torch.Tensor | None = None  # (n_ds,) uint8 EMI route with emi_precision="mixed"
 
 
 class DsChain:
@@ -35,7 +36,8 @@ class DsChain:
 
     def __init__(self, nlines: int, width: int, nimages: int, az_half_win: int, r_half_win: int,
                  p_max: float = 0.05, min_shp: int = 50, precision: str = "fp32", batch: int | None = None,
-                 device=None, timing: bool = False):
+                 device=None, timing: bool = False, emi_precision: str | None = None,
+                 cond_max: float = 1.0e4):
         self.device = torch.device(device) if device is not None else _dev.require_cuda()
         self.shape = (nlines, width, nimages)
         self.azh, self.rh = az_half_win, r_half_win
@@ -43,9 +45,16 @@ class DsChain:
         self.win = self.az_win * self.r_win
         self.p_max, self.min_shp = float(p_max), int(min_shp)
         self.prec = _lib.PREC[precision]
-        # EMI reduction in FP64 only with an FP64 Gram; FP32 otherwise (its rounding is
-        # below the FP32/BF16 coherence error it starts from)
-        self.emi_prec = _lib.PREC["fp64"] if precision == "fp64" else _lib.PREC["fp32"]
+        # EMI: FP64 with an FP64 Gram, FP32 otherwise (its rounding is below the FP32/BF16
+        # coherence error it starts from), unless asked for; "mixed" routes ill-conditioned
+        # points to FP64
+        if emi_precision is None:
+            emi_precision = "fp64" if precision == "fp64" else "fp32"
+        if emi_precision not in ("fp32", "fp64", "mixed"):
+            raise ValueError(f"emi_precision must be 'fp32', 'fp64' or 'mixed', not {emi_precision!r}")
+        self.emi_precision = emi_precision
+        self.emi_prec = _lib.PREC[emi_precision]
+        self.cond_max = float(cond_max)
         self.timing = timing
         self.npairs = nimages * (nimages - 1) // 2
         npix = nlines * width
@@ -64,6 +73,7 @@ class DsChain:
         self.ph = torch.empty((npix, nimages), dtype=torch.complex64, device=d)
         self.quality = torch.empty((npix,), dtype=torch.float32, device=d)
         self.t_coh = torch.empty((npix,), dtype=torch.float32, device=d)
+        self.route = torch.empty((npix,), dtype=torch.uint8, device=d) if emi_precision == "mixed" else None
 
     @staticmethod
     def default_batch(npix: int, nimages: int) -> int:
@@ -115,9 +125,14 @@ class DsChain:
                       self.is_shp.data_ptr(), 1, self.az_win, self.r_win, None, self.npairs, self.coh.data_ptr(),
                       self.prec, s)
             mark("coherence")
-            _lib.call("mr_emi", self.coh.data_ptr(), nb, n, 0, self.emi_prec, self.ph[b0].data_ptr(),
-                      self.quality[b0:].data_ptr(), self.t_coh[b0:].data_ptr(), self.emi_ws.data_ptr(),
-                      self.emi_ws.numel(), s)
+            if self.route is not None:
+                _lib.call("mr_emi_routed", self.coh.data_ptr(), nb, n, 0, self.cond_max, self.ph[b0].data_ptr(),
+                          self.quality[b0:].data_ptr(), self.t_coh[b0:].data_ptr(), self.route[b0:].data_ptr(),
+                          self.emi_ws.data_ptr(), self.emi_ws.numel(), s)
+            else:
+                _lib.call("mr_emi", self.coh.data_ptr(), nb, n, 0, self.emi_prec, self.ph[b0].data_ptr(),
+                          self.quality[b0:].data_ptr(), self.t_coh[b0:].data_ptr(), self.emi_ws.data_ptr(),
+                          self.emi_ws.numel(), s)
             mark("emi_tcoh")
         stage = {}
         if self.timing:
@@ -125,4 +140,5 @@ class DsChain:
             for (_, a), (name, b) in zip(ev[:-1], ev[1:]):
                 stage[name] = stage.get(name, 0.0) + a.elapsed_time(b)
         return ChainResult(n_ds, self.idx[:n_ds], self.ph[:n_ds], self.quality[:n_ds], self.t_coh[:n_ds],
-                           self.shp_num, self.is_shp, stage)
+                           self.shp_num, self.is_shp, stage,
+                           self.route[:n_ds] if self.route is not None else None)

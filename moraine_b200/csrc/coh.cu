@@ -221,8 +221,7 @@ int launch_gram(const float2* rslc, int nlines, int width, int n, const int32_t*
   const int npad = (n + 3) & ~3;
   const size_t smem = (size_t)kChunk * npad * sizeof(float2) + npad * sizeof(A) +
                       (size_t)az_win * r_win * sizeof(int);
-  MR_CUDA_TRY(cudaFuncSetAttribute(gram_kernel<A, kFull>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
+  if (int rc = allow_smem(reinterpret_cast<const void*>(gram_kernel<A, kFull>), smem)) return rc;
   const int64_t grid = std::min<int64_t>(n_pc, (int64_t)sm_count() * 8);
   gram_kernel<A, kFull><<<(unsigned)grid, kGramThreads, smem, s>>>(rslc, nlines, width, n, idx, n_pc, mask,
                                                                    mask_stride, az_win, r_win, coh, cov);

@@ -361,7 +361,7 @@ int gram_tc(const float2* rslc, int nlines, int width, int n, const int32_t* idx
   if (L.bytes > 200 * 1024) return fail(MR_ERR_UNSUPPORTED, "emperical_co_pc: window too large for the tensor-core Gram");
   const bool split = precision == MR_PREC_BF16X3;
   auto kern = split ? gram_tc_kernel<true> : gram_tc_kernel<false>;
-  MR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes));
+  if (int rc_ = allow_smem(reinterpret_cast<const void*>(kern), (size_t)(L.bytes))) return rc_;
   // one CTA per SM when it claims all 512 TMEM columns, up to four with 128 columns each
   int occ = 0;
   MR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kTcThreads, L.bytes));

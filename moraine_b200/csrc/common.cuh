@@ -42,6 +42,13 @@ inline cudaStream_t as_stream(mr_stream_t s) { return reinterpret_cast<cudaStrea
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Largest dynamic shared memory per CTA of the current device (opt-in limit).
+int smem_optin();
+
+// Lets `kernel` launch with up to the device's opt-in shared memory; fails when `bytes`
+// exceed it. Safe when several host threads launch the kernel with different sizes.
+int allow_smem(const void* kernel, size_t bytes);
+
 // Pair index of (m, j), m < j, in the row-major upper triangle of an N x N matrix
 // (the order of numpy.triu_indices(N, 1)).
 __host__ __device__ __forceinline__ int64_t triu_index(int m, int j, int n) {

@@ -33,8 +33,8 @@ namespace emi {
 // emi_fast.cu
 int fast_supported(int n);
 size_t fast_workspace_bytes(int64_t n_pc, int n);
-int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, float2* ph, float* quality,
-             float* tcoh, void* workspace, size_t workspace_bytes, cudaStream_t s);
+int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, float cond_max, float2* ph,
+             float* quality, float* tcoh, uint8_t* route, void* workspace, cudaStream_t s);
 
 namespace {
 
@@ -226,14 +226,18 @@ extern "C" size_t mr_emi_workspace_bytes(int64_t n_pc, int nimages) {
   return general_workspace_bytes(n_pc, nimages);
 }
 
-extern "C" int mr_emi(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, int precision,
-                      mr_complex64* ph, float* emi_quality, float* t_coh, void* workspace, size_t workspace_bytes,
-                      mr_stream_t stream) {
+namespace {
+
+int emi_entry(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, int precision, double cond_max,
+              mr_complex64* ph, float* emi_quality, float* t_coh, uint8_t* route, void* workspace,
+              size_t workspace_bytes, mr_stream_t stream) {
   MR_REQUIRE(nimages >= 2, "emi: nimages must be >= 2 (got %d)", nimages);
   if (nimages > MR_MAX_NIMAGES) return fail(MR_ERR_UNSUPPORTED, "emi: nimages %d > %d", nimages, MR_MAX_NIMAGES);
   MR_REQUIRE(ref >= 0 && ref < nimages, "emi: ref %d out of range [0, %d)", ref, nimages);
   MR_REQUIRE(n_pc >= 0, "emi: negative n_pc");
-  MR_REQUIRE(precision == MR_PREC_FP32 || precision == MR_PREC_FP64, "emi: precision must be FP32 or FP64");
+  MR_REQUIRE(precision == MR_PREC_FP32 || precision == MR_PREC_FP64 || precision == MR_PREC_MIXED,
+             "emi: precision must be FP32, FP64 or MIXED");
+  MR_REQUIRE(cond_max > 0, "emi: cond_max must be positive");
   if (n_pc == 0) return MR_OK;
   MR_REQUIRE(coh && ph && emi_quality, "emi: NULL pointer");
   const size_t need = mr_emi_workspace_bytes(n_pc, nimages);
@@ -244,10 +248,30 @@ extern "C" int mr_emi(const mr_complex64* coh, int64_t n_pc, int nimages, int re
   auto* c = reinterpret_cast<const float2*>(coh);
   auto* p = reinterpret_cast<float2*>(ph);
   if (fast_supported(nimages))
-    return fast_run(c, n_pc, nimages, ref, precision, p, emi_quality, t_coh, workspace, workspace_bytes, s);
+    return fast_run(c, n_pc, nimages, ref, precision, (float)std::min(cond_max, 3.0e38), p, emi_quality, t_coh,
+                    route, workspace, s);
+  // N > 128: FP64 throughout
   const size_t smem = sizeof(GeneralShared);
-  MR_CUDA_TRY(cudaFuncSetAttribute(general_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (int rc_ = allow_smem(reinterpret_cast<const void*>(general_kernel), (size_t)(smem))) return rc_;
   general_kernel<<<general_grid(n_pc), kThreads, smem, s>>>(c, n_pc, nimages, ref, p, emi_quality, t_coh,
                                                             static_cast<double*>(workspace));
-  return check_launch("emi");
+  if (int rc = check_launch("emi")) return rc;
+  if (route) MR_CUDA_TRY(cudaMemsetAsync(route, 1, (size_t)n_pc, s));
+  return MR_OK;
+}
+
+}  // namespace
+
+extern "C" int mr_emi(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, int precision,
+                      mr_complex64* ph, float* emi_quality, float* t_coh, void* workspace, size_t workspace_bytes,
+                      mr_stream_t stream) {
+  return emi_entry(coh, n_pc, nimages, ref, precision, MR_EMI_COND_MAX, ph, emi_quality, t_coh, nullptr, workspace,
+                   workspace_bytes, stream);
+}
+
+extern "C" int mr_emi_routed(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, double cond_max,
+                             mr_complex64* ph, float* emi_quality, float* t_coh, uint8_t* route, void* workspace,
+                             size_t workspace_bytes, mr_stream_t stream) {
+  return emi_entry(coh, n_pc, nimages, ref, MR_PREC_MIXED, cond_max, ph, emi_quality, t_coh, route, workspace,
+                   workspace_bytes, stream);
 }

@@ -35,7 +35,42 @@ struct GjShared {
   int piv[2];
   int piv_of_step[16 * NB];
   int step_of_row[16 * NB];
+  T part[8][16 * NB];  // row sums of |a| per warp (norm estimate)
+  T wmax[8];
 };
+
+// max_i sum_j |a_ij| over the n x n block of the register tile (the padding excluded);
+// deterministic: fixed reduction order. Whole CTA.
+template <typename T, int NB>
+__device__ T max_abs_row_sum(const T (&a)[NB][NB], int n, int tx, int ty, GjShared<T, NB>& s) {
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+#pragma unroll
+  for (int ib = 0; ib < NB; ++ib) {
+    T r = 0;
+#pragma unroll
+    for (int jb = 0; jb < NB; ++jb)
+      if (tx + 16 * jb < n) r += fabs(a[ib][jb]);
+    r += __shfl_xor_sync(0xffffffffu, r, 16);  // the two column groups tx = 2w, 2w + 1 of this warp
+    if (lane < 16) s.part[w][ty + 16 * ib] = r;
+  }
+  __syncthreads();
+  T m = 0;
+  for (int i = tid; i < n; i += blockDim.x) {
+    T r = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) r += s.part[q][i];
+    m = fmax(m, r);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) s.wmax[w] = m;
+  __syncthreads();
+  T r = s.wmax[0];
+#pragma unroll
+  for (int q = 1; q < 8; ++q) r = fmax(r, s.wmax[q]);
+  __syncthreads();
+  return r;
+}
 
 // |Gamma| of point c into the register tile (identity on the padding).
 template <typename T, int NB>
@@ -421,17 +456,41 @@ struct PointPtr {
 __host__ __device__ __forceinline__ size_t refl_off(int k, int n) { return (size_t)k * (n - 1) - (size_t)k * (k - 1) / 2; }
 
 // ----------------------------------------------------------------- kernel 1: inverse
+// Route flags of a point (sing[] in the workspace, route[] on output).
+constexpr uint8_t kRouteCond = 1;      // cond_1(|Gamma|) estimate above the threshold
+constexpr uint8_t kRouteSingular = 2;  // a zero pivot: |Gamma| singular at this precision
+
+// Points of a pass: all n_pc of the sub-batch, or list[0 .. *count) of them.
+struct PointSet {
+  const int32_t* list;
+  const int32_t* count;
+  int64_t n_pc;
+  __device__ __forceinline__ int64_t size() const { return list ? (int64_t)*count : n_pc; }
+  __device__ __forceinline__ int64_t operator[](int64_t i) const { return list ? (int64_t)list[i] : i; }
+};
+
 template <typename T, int NB>
-__global__ void __launch_bounds__(kThreads, 1) inverse_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
-                                                          unsigned char* __restrict__ ws, uint8_t* __restrict__ sing) {
+__global__ void __launch_bounds__(kThreads, 1) inverse_kernel(const float2* __restrict__ coh, PointSet pts, int n,
+                                                          unsigned char* __restrict__ ws, uint8_t* __restrict__ sing,
+                                                          float cond_max) {
   __shared__ GjShared<T, NB> gs;
   const int tid = threadIdx.x, tx = tid >> 4, ty = tid & 15;
   const int64_t npairs = (int64_t)n * (n - 1) / 2;
-  for (int64_t pt = blockIdx.x; pt < n_pc; pt += gridDim.x) {
+  const int64_t npt = pts.size();
+  for (int64_t pt = blockIdx.x; pt < npt; pt += gridDim.x) {
+    const int64_t gp = pts[pt];
     T a[NB][NB];
     unsigned used;
-    load_abs_gamma<T, NB>(a, used, coh + pt * npairs, n, tx, ty);
+    load_abs_gamma<T, NB>(a, used, coh + gp * npairs, n, tx, ty);
+    const T anorm = cond_max > 0.f ? max_abs_row_sum<T, NB>(a, n, tx, ty, gs) : T(0);
     const bool singular = gj_tile<T, NB>(a, used, n, tx, ty, gs);
+    uint8_t flag = singular ? kRouteSingular : 0;
+    if (cond_max > 0.f && !singular) {
+      // cond_1 = ||A||_1 ||inv(A)||_1 (A symmetric: row sums); the register rows of the
+      // result are the rows of inv(A) in pivot order
+      const T cond = anorm * max_abs_row_sum<T, NB>(a, n, tx, ty, gs);
+      if (!(cond <= (T)cond_max)) flag = kRouteCond;
+    }
     T* out = PointPtr<T>(ws, pt, n).ainv;
 #pragma unroll
     for (int ib = 0; ib < NB; ++ib) {
@@ -446,22 +505,23 @@ __global__ void __launch_bounds__(kThreads, 1) inverse_kernel(const float2* __re
         if (kr >= pc) out[(int64_t)kr * (kr + 1) / 2 + pc] = a[ib][jb];
       }
     }
-    if (tid == 0) sing[pt] = singular ? 1 : 0;
+    if (tid == 0) sing[pt] = flag;
     __syncthreads();
   }
 }
 
 // ----------------------------------------------------------------- kernel 2: reduction
 template <typename T>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 2) reduce_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 2) reduce_kernel(const float2* __restrict__ coh, PointSet pts, int n,
                                                          unsigned char* __restrict__ ws) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const TriShared<T> s = tri_layout<T>(smem_raw, n);
   const int tid = threadIdx.x, nt = blockDim.x;
   const int64_t npairs = (int64_t)n * (n - 1) / 2;
   const int np = n * (n + 1) / 2;
-  for (int64_t pt = blockIdx.x; pt < n_pc; pt += gridDim.x) {
-    const float2* c = coh + pt * npairs;
+  const int64_t npt = pts.size();
+  for (int64_t pt = blockIdx.x; pt < npt; pt += gridDim.x) {
+    const float2* c = coh + pts[pt] * npairs;
     PointPtr<T> w(ws, pt, n);
     // M = inv(|Gamma|) o Gamma, lower triangle packed like inv(|Gamma|) itself
     int i = 0;
@@ -501,7 +561,7 @@ __host__ __device__ inline size_t tail_warp_bytes(int n) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(32 * kTailWarps) tail_kernel(const float2* __restrict__ coh, int64_t n_pc, int n,
+__global__ void __launch_bounds__(32 * kTailWarps, 3) tail_kernel(const float2* __restrict__ coh, PointSet pts, int n,
                                                               int ref, const unsigned char* __restrict__ ws,
                                                               const uint8_t* __restrict__ sing,
                                                               float2* __restrict__ ph, float* __restrict__ quality,
@@ -520,7 +580,9 @@ __global__ void __launch_bounds__(32 * kTailWarps) tail_kernel(const float2* __r
   double2* phs = reinterpret_cast<double2*>(mine + align16(6 * (size_t)n * sizeof(T)) + align16((size_t)n * sizeof(C)));
   const int64_t npairs = (int64_t)n * (n - 1) / 2;
   const float fnan = __int_as_float(0x7fffffff);
-  for (int64_t pt = (int64_t)blockIdx.x * kTailWarps + wid; pt < n_pc; pt += (int64_t)gridDim.x * kTailWarps) {
+  const int64_t npt = pts.size();
+  for (int64_t pt = (int64_t)blockIdx.x * kTailWarps + wid; pt < npt; pt += (int64_t)gridDim.x * kTailWarps) {
+    const int64_t gp = pts[pt];
     const PointPtr<T> w(const_cast<unsigned char*>(ws), pt, n);
     // real tridiagonal: b = |e|, phases delta_{k+1} = delta_k e_k/|e_k| (warp prefix product)
     C carry = mk<T>(1, 0);
@@ -629,20 +691,20 @@ __global__ void __launch_bounds__(32 * kTailWarps) tail_kernel(const float2* __r
       __syncwarp();
     }
     // normalise to the reference image
-    const bool singular = sing[pt] != 0;
+    const bool singular = (sing[pt] & kRouteSingular) != 0;
     const C zr = z[ref];
     for (int i = lane; i < n; i += 32) {
       const C v = cmulc_t(z[i], zr);
       const double vx = v.x, vy = v.y, a = sqrt(vx * vx + vy * vy);
       float2 o = make_float2((float)(vx / a), (float)(vy / a));
       if (singular) o = make_float2(fnan, fnan);
-      ph[pt * n + i] = o;
+      ph[gp * n + i] = o;
       phs[i] = make_double2(o.x, o.y);
     }
-    if (lane == 0) quality[pt] = singular ? fnan : (float)lam;
+    if (lane == 0) quality[gp] = singular ? fnan : (float)lam;
     __syncwarp();
     if (tcoh) {  // |sum_q coh_q/|coh_q| conj(ph_m) ph_j| / n_pairs
-      const float2* c = coh + pt * npairs;
+      const float2* c = coh + gp * npairs;
       double tx = 0, ty = 0;
       int mm = 0, jj = 1 + lane;
       while (jj >= n && mm < n - 1) { mm += 1; jj = jj - n + mm + 1; }
@@ -658,7 +720,7 @@ __global__ void __launch_bounds__(32 * kTailWarps) tail_kernel(const float2* __r
       }
       tx = warp_sum(tx);
       ty = warp_sum(ty);
-      if (lane == 0) tcoh[pt] = (float)(sqrt(tx * tx + ty * ty) / (double)npairs);
+      if (lane == 0) tcoh[gp] = (float)(sqrt(tx * tx + ty * ty) / (double)npairs);
     }
     __syncwarp();
   }
@@ -673,54 +735,85 @@ int occupancy(K kernel, int threads, size_t smem) {
 }
 
 template <typename T>
-int sub_batch(int n) {
+int64_t sub_batch(int n) {
   const PointWs<T> w(n);
-  return (int)std::max<size_t>(1024, std::min<size_t>(1 << 17, (size_t)(1ull << 30) / (w.bytes + 1)));
+  return (int64_t)std::max<size_t>(1024, std::min<size_t>(1 << 17, (size_t)(1ull << 30) / (w.bytes + 1)));
+}
+
+// Workspace of one sub-batch of `sub` points: per-point state of the widest arithmetic
+// used, route flags of the FP32 and FP64 passes, the list of routed points and its count.
+struct SubWs {
+  unsigned char* pts;
+  uint8_t* sing;
+  uint8_t* sing2;
+  int32_t* list;
+  int32_t* count;
+  static size_t bytes(int64_t sub, size_t point_bytes) {
+    return align16((size_t)sub * point_bytes) + 2 * align16((size_t)sub) + align16(4 * (size_t)sub) + 16;
+  }
+  SubWs(unsigned char* ws, int64_t sub, size_t point_bytes) {
+    unsigned char* b = ws;
+    pts = b;
+    b += align16((size_t)sub * point_bytes);
+    sing = b;
+    b += align16((size_t)sub);
+    sing2 = b;
+    b += align16((size_t)sub);
+    list = reinterpret_cast<int32_t*>(b);
+    b += align16(4 * (size_t)sub);
+    count = reinterpret_cast<int32_t*>(b);
+  }
+};
+
+__global__ void route_kernel(const uint8_t* __restrict__ sing, int64_t nb, int32_t* __restrict__ list,
+                             int32_t* __restrict__ count, uint8_t* __restrict__ route) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint8_t f = sing[i];
+    if (route) route[i] = f;
+    if (f) list[atomicAdd(count, 1)] = (int32_t)i;  // list order is free: points are independent
+  }
 }
 
 template <typename T, int NB>
-int launch_inverse(const float2* coh, int64_t nb, int n, unsigned char* ws, uint8_t* sing, cudaStream_t s) {
+int launch_inverse(const float2* coh, PointSet pts, int64_t grid_cap, int n, unsigned char* ws, uint8_t* sing,
+                   float cond_max, cudaStream_t s) {
   const int occ = std::max(1, occupancy(inverse_kernel<T, NB>, kThreads, 0));
-  const int64_t grid = std::min<int64_t>(nb, (int64_t)sm_count() * occ);
-  inverse_kernel<T, NB><<<(unsigned)grid, kThreads, 0, s>>>(coh, nb, n, ws, sing);
+  const int64_t grid = std::min<int64_t>(grid_cap, (int64_t)sm_count() * occ);
+  inverse_kernel<T, NB><<<(unsigned)grid, kThreads, 0, s>>>(coh, pts, n, ws, sing, cond_max);
   return check_launch("emi inverse");
 }
 
+// One pass of the three kernels over a sub-batch (pts.list == nullptr: all pts.n_pc points;
+// else the listed ones, whose count is read on the device). cond_max > 0 flags the points
+// whose condition estimate exceeds it.
 template <typename T>
-int run_precision(const float2* coh, int64_t n_pc, int n, int ref, float2* ph, float* quality, float* tcoh,
-                  unsigned char* ws, cudaStream_t s) {
-  const int64_t sub = std::min<int64_t>(n_pc, sub_batch<T>(n));
-  uint8_t* sing = ws + align16((size_t)sub * PointWs<T>(n).bytes);
+int run_pass(const float2* c, PointSet pts, int n, int ref, float2* ph, float* quality, float* tcoh,
+             unsigned char* ws, uint8_t* sing, float cond_max, cudaStream_t s) {
+  const int64_t cap = pts.n_pc;  // grid bound: the most points this pass can see
+  int rc;
+  switch ((n + 15) / 16) {
+    case 1: case 2: rc = launch_inverse<T, 2>(c, pts, cap, n, ws, sing, cond_max, s); break;
+    case 3: rc = launch_inverse<T, 3>(c, pts, cap, n, ws, sing, cond_max, s); break;
+    case 4: rc = launch_inverse<T, 4>(c, pts, cap, n, ws, sing, cond_max, s); break;
+    case 5: rc = launch_inverse<T, 5>(c, pts, cap, n, ws, sing, cond_max, s); break;
+    case 6: rc = launch_inverse<T, 6>(c, pts, cap, n, ws, sing, cond_max, s); break;
+    case 7: rc = launch_inverse<T, 7>(c, pts, cap, n, ws, sing, cond_max, s); break;
+    default: rc = launch_inverse<T, 8>(c, pts, cap, n, ws, sing, cond_max, s); break;
+  }
+  if (rc) return rc;
   const size_t rsmem = tri_bytes<T>(n);
-  MR_CUDA_TRY(cudaFuncSetAttribute(reduce_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
+  if (int rc_ = allow_smem(reinterpret_cast<const void*>(reduce_kernel<T>), (size_t)(rsmem))) return rc_;
   const int rocc = occupancy(reduce_kernel<T>, kThreads, rsmem);
   if (rocc < 1) return fail(MR_ERR_UNSUPPORTED, "emi: %zu bytes of shared memory per CTA do not fit", rsmem);
+  reduce_kernel<T><<<(unsigned)std::min<int64_t>(cap, (int64_t)sm_count() * rocc), kThreads, rsmem, s>>>(c, pts, n,
+                                                                                                        ws);
+  if (int e = check_launch("emi reduce")) return e;
   const size_t tsmem = kTailWarps * tail_warp_bytes<T>(n);
-  MR_CUDA_TRY(cudaFuncSetAttribute(tail_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
+  if (int rc_ = allow_smem(reinterpret_cast<const void*>(tail_kernel<T>), (size_t)(tsmem))) return rc_;
   const int tocc = std::max(1, occupancy(tail_kernel<T>, 32 * kTailWarps, tsmem));
-  const int64_t npairs = (int64_t)n * (n - 1) / 2;
-  for (int64_t b0 = 0; b0 < n_pc; b0 += sub) {
-    const int64_t nb = std::min<int64_t>(sub, n_pc - b0);
-    const float2* c = coh + b0 * npairs;
-    int rc;
-    switch ((n + 15) / 16) {
-      case 1: case 2: rc = launch_inverse<T, 2>(c, nb, n, ws, sing, s); break;
-      case 3: rc = launch_inverse<T, 3>(c, nb, n, ws, sing, s); break;
-      case 4: rc = launch_inverse<T, 4>(c, nb, n, ws, sing, s); break;
-      case 5: rc = launch_inverse<T, 5>(c, nb, n, ws, sing, s); break;
-      case 6: rc = launch_inverse<T, 6>(c, nb, n, ws, sing, s); break;
-      case 7: rc = launch_inverse<T, 7>(c, nb, n, ws, sing, s); break;
-      default: rc = launch_inverse<T, 8>(c, nb, n, ws, sing, s); break;
-    }
-    if (rc) return rc;
-    reduce_kernel<T><<<(unsigned)std::min<int64_t>(nb, (int64_t)sm_count() * rocc), kThreads, rsmem, s>>>(c, nb, n, ws);
-    if (int e = check_launch("emi reduce")) return e;
-    const int64_t tgrid = std::min<int64_t>((nb + kTailWarps - 1) / kTailWarps, (int64_t)sm_count() * tocc);
-    tail_kernel<T><<<(unsigned)tgrid, 32 * kTailWarps, tsmem, s>>>(c, nb, n, ref, ws, sing, ph + b0 * n,
-                                                                    quality + b0, tcoh ? tcoh + b0 : nullptr);
-    if (int e = check_launch("emi tail")) return e;
-  }
-  return MR_OK;
+  const int64_t tgrid = std::min<int64_t>((cap + kTailWarps - 1) / kTailWarps, (int64_t)sm_count() * tocc);
+  tail_kernel<T><<<(unsigned)tgrid, 32 * kTailWarps, tsmem, s>>>(c, pts, n, ref, ws, sing, ph, quality, tcoh);
+  return check_launch("emi tail");
 }
 
 }  // namespace
@@ -730,16 +823,44 @@ int fast_supported(int n) { return n >= 2 && n <= kMaxFastN; }
 size_t fast_workspace_bytes(int64_t n_pc, int n) {
   const int64_t s32 = std::min<int64_t>(n_pc, sub_batch<float>(n));
   const int64_t s64 = std::min<int64_t>(n_pc, sub_batch<double>(n));
-  return std::max(align16((size_t)s32 * PointWs<float>(n).bytes) + (size_t)s32,
-                  align16((size_t)s64 * PointWs<double>(n).bytes) + (size_t)s64);
+  return std::max(SubWs::bytes(s32, PointWs<float>(n).bytes), SubWs::bytes(s64, PointWs<double>(n).bytes));
 }
 
-int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, float2* ph, float* quality,
-             float* tcoh, void* workspace, size_t workspace_bytes, cudaStream_t s) {
-  (void)workspace_bytes;
+int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, float cond_max, float2* ph,
+             float* quality, float* tcoh, uint8_t* route, void* workspace, cudaStream_t s) {
   auto* ws = static_cast<unsigned char*>(workspace);
-  if (precision == MR_PREC_FP64) return run_precision<double>(coh, n_pc, n, ref, ph, quality, tcoh, ws, s);
-  return run_precision<float>(coh, n_pc, n, ref, ph, quality, tcoh, ws, s);
+  const bool f64 = precision == MR_PREC_FP64;
+  const bool mixed = precision == MR_PREC_MIXED;
+  // a mixed sub-batch must hold its points in FP64 when all of them are routed
+  const int64_t sub = std::min<int64_t>(n_pc, (f64 || mixed) ? sub_batch<double>(n) : sub_batch<float>(n));
+  const SubWs w(ws, sub, f64 || mixed ? PointWs<double>(n).bytes : PointWs<float>(n).bytes);
+  const int64_t npairs = (int64_t)n * (n - 1) / 2;
+  for (int64_t b0 = 0; b0 < n_pc; b0 += sub) {
+    const int64_t nb = std::min<int64_t>(sub, n_pc - b0);
+    const float2* c = coh + b0 * npairs;
+    float2* p = ph + b0 * n;
+    float* q = quality + b0;
+    float* t = tcoh ? tcoh + b0 : nullptr;
+    const PointSet all{nullptr, nullptr, nb};
+    int rc;
+    if (f64) {
+      rc = run_pass<double>(c, all, n, ref, p, q, t, w.pts, w.sing, 0.f, s);
+      if (!rc && route) MR_CUDA_TRY(cudaMemsetAsync(route + b0, 1, (size_t)nb, s));
+    } else {
+      rc = run_pass<float>(c, all, n, ref, p, q, t, w.pts, w.sing, mixed ? cond_max : 0.f, s);
+      if (!rc && mixed) {
+        MR_CUDA_TRY(cudaMemsetAsync(w.count, 0, sizeof(int32_t), s));
+        const int grid = (int)std::min<int64_t>((nb + 255) / 256, (int64_t)sm_count() * 8);
+        route_kernel<<<grid, 256, 0, s>>>(w.sing, nb, w.list, w.count, route ? route + b0 : nullptr);
+        rc = check_launch("emi route");
+        if (!rc) rc = run_pass<double>(c, PointSet{w.list, w.count, nb}, n, ref, p, q, t, w.pts, w.sing2, 0.f, s);
+      } else if (!rc && route) {
+        MR_CUDA_TRY(cudaMemsetAsync(route + b0, 0, (size_t)nb, s));
+      }
+    }
+    if (rc) return rc;
+  }
+  return MR_OK;
 }
 
 }  // namespace emi

@@ -338,8 +338,7 @@ extern "C" int mr_ks_test(const float* rmli, int nlines, int width, int nimages,
   // host staging of the table; the launch copies it into the kernel's parameter buffer
   static thread_local KsTable tab_local;
   fill_table(tab_local, nimages, p_max);
-  MR_CUDA_TRY(cudaFuncSetAttribute(ks_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)plan.smem));
+  if (int rc_ = allow_smem(reinterpret_cast<const void*>(ks_merge_kernel), (size_t)(plan.smem))) return rc_;
   const int64_t tiles = (int64_t)((nlines + plan.th - 1) / plan.th) * ((width + plan.tw - 1) / plan.tw);
   MR_REQUIRE(tiles < (1ll << 31), "ks_test: image too large");
   ks_merge_kernel<<<(unsigned)tiles, kKsThreads, plan.smem, s>>>(

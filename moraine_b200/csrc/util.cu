@@ -36,6 +36,31 @@ int sm_count() {
   return cached[dev];
 }
 
+int smem_optin() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  if (cached[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) n = 0;
+    cached[dev] = n;
+  }
+  return cached[dev];
+}
+
+int allow_smem(const void* kernel, size_t bytes) {
+  const int optin = smem_optin();
+  if (optin <= 0) return fail(MR_ERR_CUDA, "cannot query the shared-memory limit of the device");
+  cudaFuncAttributes fa;
+  MR_CUDA_TRY(cudaFuncGetAttributes(&fa, kernel));
+  const int cap = optin - (int)fa.sharedSizeBytes;  // dynamic share beside the kernel's static one
+  if (bytes > (size_t)cap) return fail(MR_ERR_UNSUPPORTED, "%zu bytes of shared memory per CTA > %d", bytes, cap);
+  // the device limit, not this launch's size: threads that launch the kernel with other
+  // sizes at the same time all write the same value
+  MR_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
+  return MR_OK;
+}
+
 }  // namespace mr
 
 extern "C" const char* mr_last_error(void) { return mr::g_last_error; }

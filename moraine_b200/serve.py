@@ -40,7 +40,8 @@ class TileRequest:
     r_half_win: int = 5
     p_max: float = 0.05
     min_shp: int = 50
-    precision: str = "fp32"
+    precision: str = "fp64"             # coherence Gram arithmetic
+    emi_precision: str | None = None    # EMI arithmetic (default: follows the Gram)
     request_id: int = 0
     arrival: float | None = None   # time.perf_counter() of arrival; set by submit() if None
 
@@ -199,12 +200,12 @@ class DsServer:
 
     def _run_chain(self, req: TileRequest, plan: dict, stream) -> dict:
         nl, w, n = req.rslc.shape
-        key = (nl, w, n, req.az_half_win, req.r_half_win, req.p_max, req.min_shp, req.precision)
+        key = (nl, w, n, req.az_half_win, req.r_half_win, req.p_max, req.min_shp, req.precision, req.emi_precision)
         chain = plan.get(key)
         if chain is None:
             plan.clear()  # one plan per slot: a new shape frees the previous buffers
             chain = DsChain(nl, w, n, req.az_half_win, req.r_half_win, req.p_max, req.min_shp,
-                            precision=req.precision, device=self.device)
+                            precision=req.precision, emi_precision=req.emi_precision, device=self.device)
             plan[key] = chain
         x = req.rslc
         if not x.is_cuda:

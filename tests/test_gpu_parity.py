@@ -153,6 +153,66 @@ def test_emi_vs_fp64_oracle(cuda, name, size, precision):
     assert err[well].max(initial=0) < 1e-3
 
 
+def _abs_gamma_cond(coh):
+    g = np.abs(O.uncompress_coh(coh.astype(np.complex128)))
+    return np.linalg.cond(g, 1)
+
+
+@pytest.mark.parametrize("name,size", [("c2", 40), ("c3", 24), ("c1", 32)])
+def test_emi_mixed_routing(cuda, name, size):
+    """Mixed precision: unrouted points equal the FP32 run and routed points the FP64 run, bit
+    for bit; the route follows cond_1(|Gamma|)."""
+    cfg = CONFIGS[name].scaled(nlines=size, width=size, nimages=min(100, CONFIGS[name].nimages))
+    z = make_stack(cfg).numpy()
+    p = O.ks_test(O.intensity(z), cfg.az_half_win, cfg.r_half_win)
+    is_shp, num = O.select_shp(p, cfg.p_max)
+    idx, pc = O.ds_candidates(is_shp, num, 1)
+    coh = torch.from_numpy(O.emperical_co_pc(z, idx, pc).astype(np.complex64)).to(cuda)
+    n = O.nimage_from_npair(coh.shape[1])
+    from moraine_b200.pl import _emi_device
+    runs = {prec: _emi_device(coh, n, 0, True, prec) for prec in ("fp32", "fp64")}
+    route = torch.empty((coh.shape[0],), dtype=torch.uint8, device=cuda)
+    mixed = _emi_device(coh, n, 0, True, "mixed", cond_max=1e4, route=route)
+    r = route.cpu().numpy()
+    assert set(np.unique(r)) <= {0, 1, 2}
+    assert (r == 0).any() and (r != 0).any()
+    for k in range(3):
+        m = mixed[k].cpu()
+        for sel, prec in ((r == 0, "fp32"), (r != 0, "fp64")):
+            a = m[torch.from_numpy(sel)].view(torch.int32 if m.dtype == torch.float32 else torch.float32)
+            b = runs[prec][k].cpu()[torch.from_numpy(sel)]
+            b = b.view(torch.int32 if b.dtype == torch.float32 else torch.float32)
+            assert torch.equal(a, b), (name, k, prec)
+    # the estimate is cond_1(|Gamma|) itself, evaluated in FP32
+    cond = _abs_gamma_cond(coh.cpu().numpy())
+    assert np.all(cond[r == 1] > 1e4 / 2)
+    assert np.all((cond[r == 0] < 1e4 * 2) | ~np.isfinite(cond[r == 0]))
+    # everything routed by condition / nothing routed
+    route.fill_(9)
+    _emi_device(coh, n, 0, False, "mixed", cond_max=1.0, route=route)
+    assert torch.all(route.cpu() != 0)
+    _emi_device(coh, n, 0, False, "mixed", cond_max=1e30, route=route)
+    assert not torch.any(route.cpu() == 1)
+    # python API
+    ph, q, rt = mb.emi(coh.cpu().numpy(), precision="mixed", return_route=True)
+    np.testing.assert_array_equal(rt, r)
+    with pytest.raises(ValueError):
+        mb.emi(coh.cpu().numpy(), precision="fp32", return_route=True)
+
+
+def test_chain_mixed_route(cuda):
+    cfg = CONFIGS["c3"].scaled(nlines=24, width=24, nimages=64)
+    z = make_stack(cfg, device=cuda)
+    ch = DsChain(24, 24, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, 1, device=cuda,
+                 emi_precision="mixed")
+    res = ch.run(z)
+    ref = DsChain(24, 24, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, 1, device=cuda).run(z)
+    assert res.route is not None and res.route.shape == (res.n_ds,)
+    keep = res.route == 0
+    assert keep.any()
+    assert torch.equal(res.ph[keep], ref.ph[keep])
+
+
 def test_emi_edges(cuda):
     # N = 2 and N = 3 with exact coherence, reference image other than 0
     for n in (2, 3, 5):
