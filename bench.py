@@ -123,9 +123,11 @@ def measured_peaks() -> dict:
 
 DTYPE = {"fp32": "f32", "bf16": "bf16 Gram, f32 EMI", "bf16x3": "bf16x3 Gram, f32 EMI", "fp64": "f64"}
 
-# DRAM bytes per DS point of one mr_emi call (inverse + reduce + tail kernels), from the
-# ncu capture of the 2000 x 2000 x 100 scene's EMI sub-batch (N = 100)
-EMI_TRAFFIC_PER_POINT = {100: None}
+# DRAM bytes per DS point of one mr_emi call (inverse + reduce + tail kernels), by (N, EMI
+# arithmetic): dram__bytes_read.sum + dram__bytes_write.sum of the three kernels over one
+# sub-batch, from ncu captures of the c2 scene model at N = 100 (FP64: 3.117 GB / 8,743
+# points; FP32: 4.195 GB / 17,485 points); the traffic scales with the points processed
+EMI_TRAFFIC_PER_POINT = {(100, "fp64"): 356_500, (100, "fp32"): 239_900}
 
 
 def fp32_simt_peak(dev) -> float:
@@ -194,7 +196,7 @@ def stage_rooflines(cfg, stage: dict, n_ds: int, res, peaks: dict, fp32: float, 
         calls = -(-n_ds // chain.batch)
         flops = n_ds * (2.7 * n ** 3 + 80 * n ** 2)
         tf = flops / (ms / 1e3) / 1e12
-        tpp = EMI_TRAFFIC_PER_POINT.get(n)
+        tpp = EMI_TRAFFIC_PER_POINT.get((n, chain.emi_precision))
         f64 = chain.emi_precision == "fp64" or n > 128
         peak = fp32 / 2 if f64 else fp32  # the FP64 pipe of B200 runs at half the FP32 rate
         out["emi_tcoh"] = {"kernel": "mr_emi: inverse_kernel + reduce_kernel + tail_kernel", "bound":
