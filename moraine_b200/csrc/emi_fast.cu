@@ -29,27 +29,37 @@ namespace {
 
 constexpr int kMaxFastN = 128;
 
-template <typename T, int NB>
+// Gauss-Jordan thread grid: 16 row lanes (ty) x CX column groups (tx), thread tid = 16 tx + ty;
+// thread (tx, ty) holds rows ty + 16 ib (ib < NB) and columns tx + CX jb (jb < NC).
+template <int NB, int CX>
+struct GjGrid {
+  static constexpr int NC = (16 * NB + CX - 1) / CX;
+  static constexpr int kThreads = 16 * CX;
+  static constexpr int kWarps = kThreads / 32;
+};
+
+template <typename T, int NB, int CX>
 struct GjShared {
   T col[2][16 * NB];
   int piv[2];
   int piv_of_step[16 * NB];
   int step_of_row[16 * NB];
-  T part[8][16 * NB];  // row sums of |a| per warp (norm estimate)
-  T wmax[8];
+  T part[GjGrid<NB, CX>::kWarps][16 * NB];  // row sums of |a| per warp (norm estimate)
+  T wmax[GjGrid<NB, CX>::kWarps];
 };
 
 // max_i sum_j |a_ij| over the n x n block of the register tile (the padding excluded);
 // deterministic: fixed reduction order. Whole CTA.
-template <typename T, int NB>
-__device__ T max_abs_row_sum(const T (&a)[NB][NB], int n, int tx, int ty, GjShared<T, NB>& s) {
+template <typename T, int NB, int CX>
+__device__ T max_abs_row_sum(const T (&a)[NB][GjGrid<NB, CX>::NC], int n, int tx, int ty, GjShared<T, NB, CX>& s) {
+  constexpr int NC = GjGrid<NB, CX>::NC, W = GjGrid<NB, CX>::kWarps;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
 #pragma unroll
   for (int ib = 0; ib < NB; ++ib) {
     T r = 0;
 #pragma unroll
-    for (int jb = 0; jb < NB; ++jb)
-      if (tx + 16 * jb < n) r += fabs(a[ib][jb]);
+    for (int jb = 0; jb < NC; ++jb)
+      if (tx + CX * jb < n) r += fabs(a[ib][jb]);
     r += __shfl_xor_sync(0xffffffffu, r, 16);  // the two column groups tx = 2w, 2w + 1 of this warp
     if (lane < 16) s.part[w][ty + 16 * ib] = r;
   }
@@ -58,7 +68,7 @@ __device__ T max_abs_row_sum(const T (&a)[NB][NB], int n, int tx, int ty, GjShar
   for (int i = tid; i < n; i += blockDim.x) {
     T r = 0;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) r += s.part[q][i];
+    for (int q = 0; q < W; ++q) r += s.part[q][i];
     m = fmax(m, r);
   }
 #pragma unroll
@@ -67,23 +77,24 @@ __device__ T max_abs_row_sum(const T (&a)[NB][NB], int n, int tx, int ty, GjShar
   __syncthreads();
   T r = s.wmax[0];
 #pragma unroll
-  for (int q = 1; q < 8; ++q) r = fmax(r, s.wmax[q]);
+  for (int q = 1; q < W; ++q) r = fmax(r, s.wmax[q]);
   __syncthreads();
   return r;
 }
 
 // |Gamma| of point c into the register tile (identity on the padding).
-template <typename T, int NB>
-__device__ __forceinline__ void load_abs_gamma(T (&a)[NB][NB], unsigned& used, const float2* __restrict__ c, int n,
-                                               int tx, int ty) {
+template <typename T, int NB, int CX>
+__device__ __forceinline__ void load_abs_gamma(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned& used,
+                                               const float2* __restrict__ c, int n, int tx, int ty) {
+  constexpr int NC = GjGrid<NB, CX>::NC;
   used = 0;
 #pragma unroll
   for (int ib = 0; ib < NB; ++ib) {
     const int i = ty + 16 * ib;
     if (i >= n) used |= 1u << ib;  // padding rows never pivot
 #pragma unroll
-    for (int jb = 0; jb < NB; ++jb) {
-      const int j = tx + 16 * jb;
+    for (int jb = 0; jb < NC; ++jb) {
+      const int j = tx + CX * jb;
       T v = (i == j) ? T(1) : T(0);
       if (i < n && j < n && i != j) {
         const float2 g = c[i < j ? triu_index(i, j, n) : triu_index(j, i, n)];
@@ -97,14 +108,15 @@ __device__ __forceinline__ void load_abs_gamma(T (&a)[NB][NB], unsigned& used, c
 __device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double recip(double x) { return 1.0 / x; }
 
-// One Gauss-Jordan step k = 16 KB + kt on the register tile; KB is a compile-time column
+// One Gauss-Jordan step k = CX KB + kt on the register tile; KB is a compile-time column
 // slot, so the pivot column is read and rewritten without dynamic register indexing.
-template <typename T, int NB, int KB>
-__device__ __forceinline__ void gj_step(T (&a)[NB][NB], unsigned& used, int k, int tx, int ty, bool& singular,
-                                        GjShared<T, NB>& s) {
+template <typename T, int NB, int CX, int KB>
+__device__ __forceinline__ void gj_step(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned& used, int k, int tx, int ty,
+                                        bool& singular, GjShared<T, NB, CX>& s) {
+  constexpr int NC = GjGrid<NB, CX>::NC;
   const int tid = threadIdx.x;
   const int buf = k & 1;
-  const bool owner = tx == (k & 15);
+  const bool owner = tx == (k % CX);
   if (owner) {  // the half-warp owning column k: publish it, find the pivot
     const unsigned half = (tx & 1) ? 0xFFFF0000u : 0x0000FFFFu;
     T best = T(-1);
@@ -133,12 +145,12 @@ __device__ __forceinline__ void gj_step(T (&a)[NB][NB], unsigned& used, int k, i
   if (tid == 0) { s.piv_of_step[k] = p; s.step_of_row[p] = k; }
   const int pl = p & 15;
   // pivot row (scaled) from row lane pl of this column group; p >> 4 is CTA-uniform
-  T r[NB];
+  T r[NC];
   switch (p >> 4) {
 #define MR_GJ_ROW(PB)                                                                  \
   case PB:                                                                             \
     if (PB < NB) {                                                                     \
-      _Pragma("unroll") for (int jb = 0; jb < NB; ++jb) r[jb] =                        \
+      _Pragma("unroll") for (int jb = 0; jb < NC; ++jb) r[jb] =                        \
           __shfl_sync(0xffffffffu, a[PB < NB ? PB : 0][jb], pl, 16) * rp;              \
     }                                                                                  \
     break;
@@ -154,30 +166,32 @@ __device__ __forceinline__ void gj_step(T (&a)[NB][NB], unsigned& used, int k, i
     const T fi = s.col[buf][i];
     const T f = (i == p) ? pv - T(1) : fi;
 #pragma unroll
-    for (int jb = 0; jb < NB; ++jb) a[ib][jb] -= f * r[jb];
+    for (int jb = 0; jb < NC; ++jb) a[ib][jb] -= f * r[jb];
     if (owner) a[ib][KB] = (i == p) ? rp : -fi * rp;
   }
 }
 
 // In-place Gauss-Jordan inverse with partial pivoting on the register tile. Returns true
 // when a zero pivot was met (the matrix is singular).
-template <typename T, int NB>
-__device__ bool gj_tile(T (&a)[NB][NB], unsigned used, int n, int tx, int ty, GjShared<T, NB>& s) {
+template <typename T, int NB, int CX>
+__device__ bool gj_tile(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned used, int n, int tx, int ty,
+                        GjShared<T, NB, CX>& s) {
+  constexpr int NC = GjGrid<NB, CX>::NC;
   bool singular = false;
 #pragma unroll
-  for (int kb = 0; kb < NB; ++kb) {
-    for (int kt = 0; kt < 16; ++kt) {
-      const int k = 16 * kb + kt;
+  for (int kb = 0; kb < NC; ++kb) {
+    for (int kt = 0; kt < CX; ++kt) {
+      const int k = CX * kb + kt;
       if (k >= n) break;
       switch (kb) {  // compile-time slot (the loop over kb is unrolled)
-        case 0: gj_step<T, NB, 0>(a, used, k, tx, ty, singular, s); break;
-        case 1: if (NB > 1) gj_step<T, NB, (1 < NB ? 1 : 0)>(a, used, k, tx, ty, singular, s); break;
-        case 2: if (NB > 2) gj_step<T, NB, (2 < NB ? 2 : 0)>(a, used, k, tx, ty, singular, s); break;
-        case 3: if (NB > 3) gj_step<T, NB, (3 < NB ? 3 : 0)>(a, used, k, tx, ty, singular, s); break;
-        case 4: if (NB > 4) gj_step<T, NB, (4 < NB ? 4 : 0)>(a, used, k, tx, ty, singular, s); break;
-        case 5: if (NB > 5) gj_step<T, NB, (5 < NB ? 5 : 0)>(a, used, k, tx, ty, singular, s); break;
-        case 6: if (NB > 6) gj_step<T, NB, (6 < NB ? 6 : 0)>(a, used, k, tx, ty, singular, s); break;
-        default: if (NB > 7) gj_step<T, NB, (7 < NB ? 7 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 0: gj_step<T, NB, CX, 0>(a, used, k, tx, ty, singular, s); break;
+        case 1: if (NC > 1) gj_step<T, NB, CX, (1 < NC ? 1 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 2: if (NC > 2) gj_step<T, NB, CX, (2 < NC ? 2 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 3: if (NC > 3) gj_step<T, NB, CX, (3 < NC ? 3 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 4: if (NC > 4) gj_step<T, NB, CX, (4 < NC ? 4 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 5: if (NC > 5) gj_step<T, NB, CX, (5 < NC ? 5 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 6: if (NC > 6) gj_step<T, NB, CX, (6 < NC ? 6 : 0)>(a, used, k, tx, ty, singular, s); break;
+        default: if (NC > 7) gj_step<T, NB, CX, (7 < NC ? 7 : 0)>(a, used, k, tx, ty, singular, s); break;
       }
     }
   }
@@ -469,26 +483,27 @@ struct PointSet {
   __device__ __forceinline__ int64_t operator[](int64_t i) const { return list ? (int64_t)list[i] : i; }
 };
 
-template <typename T, int NB>
-__global__ void __launch_bounds__(kThreads, 1) inverse_kernel(const float2* __restrict__ coh, PointSet pts, int n,
+template <typename T, int NB, int CX>
+__global__ void __launch_bounds__(16 * CX, 1) inverse_kernel(const float2* __restrict__ coh, PointSet pts, int n,
                                                           unsigned char* __restrict__ ws, uint8_t* __restrict__ sing,
                                                           float cond_max) {
-  __shared__ GjShared<T, NB> gs;
+  constexpr int NC = GjGrid<NB, CX>::NC;
+  __shared__ GjShared<T, NB, CX> gs;
   const int tid = threadIdx.x, tx = tid >> 4, ty = tid & 15;
   const int64_t npairs = (int64_t)n * (n - 1) / 2;
   const int64_t npt = pts.size();
   for (int64_t pt = blockIdx.x; pt < npt; pt += gridDim.x) {
     const int64_t gp = pts[pt];
-    T a[NB][NB];
+    T a[NB][NC];
     unsigned used;
-    load_abs_gamma<T, NB>(a, used, coh + gp * npairs, n, tx, ty);
-    const T anorm = cond_max > 0.f ? max_abs_row_sum<T, NB>(a, n, tx, ty, gs) : T(0);
-    const bool singular = gj_tile<T, NB>(a, used, n, tx, ty, gs);
+    load_abs_gamma<T, NB, CX>(a, used, coh + gp * npairs, n, tx, ty);
+    const T anorm = cond_max > 0.f ? max_abs_row_sum<T, NB, CX>(a, n, tx, ty, gs) : T(0);
+    const bool singular = gj_tile<T, NB, CX>(a, used, n, tx, ty, gs);
     uint8_t flag = singular ? kRouteSingular : 0;
     if (cond_max > 0.f && !singular) {
       // cond_1 = ||A||_1 ||inv(A)||_1 (A symmetric: row sums); the register rows of the
       // result are the rows of inv(A) in pivot order
-      const T cond = anorm * max_abs_row_sum<T, NB>(a, n, tx, ty, gs);
+      const T cond = anorm * max_abs_row_sum<T, NB, CX>(a, n, tx, ty, gs);
       if (!(cond <= (T)cond_max)) flag = kRouteCond;
     }
     T* out = PointPtr<T>(ws, pt, n).ainv;
@@ -498,8 +513,8 @@ __global__ void __launch_bounds__(kThreads, 1) inverse_kernel(const float2* __re
       if (r0 >= n) continue;
       const int kr = gs.step_of_row[r0];
 #pragma unroll
-      for (int jb = 0; jb < NB; ++jb) {
-        const int c0 = tx + 16 * jb;
+      for (int jb = 0; jb < NC; ++jb) {
+        const int c0 = tx + CX * jb;
         if (c0 >= n) continue;
         const int pc = gs.piv_of_step[c0];
         if (kr >= pc) out[(int64_t)kr * (kr + 1) / 2 + pc] = a[ib][jb];
@@ -774,12 +789,19 @@ __global__ void route_kernel(const uint8_t* __restrict__ sing, int64_t nb, int32
   }
 }
 
+// Column groups of the Gauss-Jordan grid. 32 groups (512 threads, half the registers per
+// thread) measured no faster than 16 in FP32 or FP64: one point per SM either way, and its
+// serial pivot steps set the pace.
+template <typename T>
+constexpr int gj_cx() { return 16; }
+
 template <typename T, int NB>
 int launch_inverse(const float2* coh, PointSet pts, int64_t grid_cap, int n, unsigned char* ws, uint8_t* sing,
                    float cond_max, cudaStream_t s) {
-  const int occ = std::max(1, occupancy(inverse_kernel<T, NB>, kThreads, 0));
+  constexpr int CX = gj_cx<T>();
+  const int occ = std::max(1, occupancy(inverse_kernel<T, NB, CX>, 16 * CX, 0));
   const int64_t grid = std::min<int64_t>(grid_cap, (int64_t)sm_count() * occ);
-  inverse_kernel<T, NB><<<(unsigned)grid, kThreads, 0, s>>>(coh, pts, n, ws, sing, cond_max);
+  inverse_kernel<T, NB, CX><<<(unsigned)grid, 16 * CX, 0, s>>>(coh, pts, n, ws, sing, cond_max);
   return check_launch("emi inverse");
 }
 
