@@ -125,7 +125,7 @@ __device__ __forceinline__ void gj_step(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned
     for (int ib = 0; ib < NB; ++ib) {
       const T v = a[ib][KB];
       s.col[buf][ty + 16 * ib] = v;
-      const T av = fabs(v);
+      const T av = fabs(v) == fabs(v) ? fabs(v) : T(-0.5);  // NaN ranks last but is taken
       if (!(used & (1u << ib)) && av > best) { best = av; bi = ty + 16 * ib; }
     }
 #pragma unroll
