@@ -279,8 +279,9 @@ template <typename C> __device__ __forceinline__ void rank2(C& a, C ui, C wj, C 
 //   2. phase 1: step k-1's rank-2 update on the lower triangle of rows >= k+1 and the row
 //      part of (M u_k)_i = sum_{j<=i} M_ij u_j;
 //   3. phase 2: the column part sum_{j>i} conj(M_ji) u_j, then p_k = tau_k M u_k.
-// Rows are handled in mirrored pairs (i, n+k-i) by 4 threads each, which gives every
-// thread the same number of elements in both phases. The packed triangle halves the
+// Rows are handled in mirrored pairs (i, n+k-i) by groups of 4 to 32 threads (as many as
+// keep the CTA busy while the trailing matrix shrinks), which gives every thread of a step
+// the same number of elements in both phases. The packed triangle halves the
 // shared memory of full storage, so twice as many points are in flight per SM.
 template <typename T>
 __device__ void tridiag_packed(const TriShared<T>& s, int n) {
@@ -288,8 +289,6 @@ __device__ void tridiag_packed(const TriShared<T>& s, int n) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   C* L = s.L;
   C* wp = s.vec + 2 * n;  // w_{k-1}
-  const int pq = tid >> 2, sub = tid & 3;  // row pair, sub-thread of the quad
-  const unsigned quad = 0xFu << (lane & ~3);
   for (int k = 0; k + 2 < n; ++k) {
     C* up = s.vec + ((k + 1) & 1) * n;  // u_{k-1}
     C* uc = s.vec + (k & 1) * n;        // u_k
@@ -352,6 +351,11 @@ __device__ void tridiag_packed(const TriShared<T>& s, int n) {
     const T tau_k = s.tau[k];
     const int m = n - k - 1;         // rows k+1..n-1
     const int npair = (m + 1) >> 1;  // mirrored pairs (the middle row of an odd m alone)
+    // G threads per pair, as many as keep every thread of the CTA busy (4 to 32)
+    int G = 4;
+    while (G < 32 && npair * G * 2 <= (int)blockDim.x) G <<= 1;
+    const int pq = tid / G, sub = tid & (G - 1);
+    const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u) << (lane & ~(G - 1));
     const bool active = (pending || tau_k != T(0)) && pq < npair;
     const int i1 = k + 1 + pq, i2 = n - 1 - pq;
     const bool two = i2 != i1;
@@ -366,7 +370,7 @@ __device__ void tridiag_packed(const TriShared<T>& s, int n) {
         C upi = mk<T>(0, 0), wpi = mk<T>(0, 0);
         if (pending) { upi = up[i]; wpi = wp[i]; }
         C acc = mk<T>(0, 0);
-        for (int j = k + 1 + sub; j <= i; j += 4) {
+        for (int j = k + 1 + sub; j <= i; j += G) {
           C a = row[j];
           if (pending) { rank2(a, upi, wp[j], wpi, up[j]); row[j] = a; }
           const C u = uc[j];
@@ -384,16 +388,16 @@ __device__ void tridiag_packed(const TriShared<T>& s, int n) {
         if (r && !two) break;
         const int i = r ? i2 : i1;
         C acc = r ? rs2 : rs1;
-        for (int j = i + 1 + sub; j < n; j += 4) {
+        for (int j = i + 1 + sub; j < n; j += G) {
           const C a = L[tri(j) + i];  // M_ji, lower triangle
           const C u = uc[j];
           acc.x += a.x * u.x + a.y * u.y;  // conj(M_ji) u_j
           acc.y += a.x * u.y - a.y * u.x;
         }
-        acc.x += __shfl_xor_sync(quad, acc.x, 1);
-        acc.y += __shfl_xor_sync(quad, acc.y, 1);
-        acc.x += __shfl_xor_sync(quad, acc.x, 2);
-        acc.y += __shfl_xor_sync(quad, acc.y, 2);
+        for (int o = 1; o < G; o <<= 1) {
+          acc.x += __shfl_xor_sync(gmask, acc.x, o);
+          acc.y += __shfl_xor_sync(gmask, acc.y, o);
+        }
         if (sub == 0) s.pv[(k & 1) * n + i] = mk<T>(tau_k * acc.x, tau_k * acc.y);
       }
     }
