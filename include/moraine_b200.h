@@ -153,6 +153,25 @@ int mr_uncompress_coh(const mr_complex64* coh, int64_t n, int nimages,
                       const int32_t* image_pairs, int n_pairs, mr_complex64* out,
                       mr_stream_t stream);
 
+/* ---------------------------------------------------------------- GAMMA ingest
+ * Sample types of GAMMA rasters (moraine/gamma_.py:24-31: float, fcomplex, int, double). */
+enum {
+  MR_GAMMA_FLOAT = 0,    /* big-endian float32 */
+  MR_GAMMA_FCOMPLEX = 1, /* big-endian complex64 (real, imaginary) */
+  MR_GAMMA_INT = 2,      /* big-endian int32 */
+  MR_GAMMA_DOUBLE = 3,   /* big-endian float64 */
+};
+
+/* Bytes per sample of a GAMMA dtype (0 for an unknown one). */
+size_t mr_gamma_sample_bytes(int dtype);
+
+/* Replaces the decode step of moraine.gamma_.read_gamma_image / read_gamma_pdata
+ * (moraine/gamma_.py:46-56, :75-84): n big-endian samples at `be` (device memory, the
+ * file's bytes as read) to native samples at out[i * out_stride], |x| < 1e-30 -> NaN
+ * (NaN + NaN j for fcomplex; int unchanged). Both buffers aligned to the sample size. */
+int mr_gamma_decode(const void* be, int64_t n, int dtype, void* out, int64_t out_stride,
+                    mr_stream_t stream);
+
 /* ---------------------------------------------------------------- phase linking
  * Replaces moraine.pl.emi (moraine/pl.py:68-77; GPU :19-42, CPU :46-65): for every
  * point, M = inv(|Gamma|) o Gamma from the full-triangle compressed coherence, its

@@ -27,6 +27,8 @@ _SIGNATURES = {
     "mr_last_error": (ctypes.c_char_p, []),
     "mr_abi_version": (c_int, []),
     "mr_kernel_launches": (ctypes.c_uint64, []),
+    "mr_gamma_sample_bytes": (c_size_t, [c_int]),
+    "mr_gamma_decode": (c_int, [P, c_int64, c_int, P, c_int64, P]),
     "mr_intensity": (c_int, [P, c_int64, P, P]),
     "mr_ks_workspace_bytes": (c_size_t, [c_int, c_int, c_int]),
     "mr_ks_test": (c_int, [P, c_int, c_int, c_int, c_int, c_int, P, P, c_double, P, P, P, c_size_t, P]),

@@ -245,3 +245,30 @@ def chain(rslc, az_half_win, r_half_win, p_max=0.05, min_shp=50, nthreads: int =
     tc = ds_temp_coh(coh.astype(np.complex64), ph.astype(np.complex64), nthreads=nthreads)
     return dict(p=p, is_shp=is_shp, shp_num=shp_num, idx=idx, coh=coh, ph=ph, quality=q, gap=gap, cond=cond,
                 t_coh=tc)
+
+
+# ----------------------------------------------------------------------------- GAMMA rasters
+GAMMA_TYPES = {"float": ">f4", "fcomplex": ">c8", "int": ">i4", "double": ">f8"}
+
+
+def gamma_decode(raw: bytes, dtype: str) -> np.ndarray:
+    """moraine/gamma_.py:46-56: big-endian samples to native, |x| < 1e-30 -> NaN (not for int)."""
+    dt = GAMMA_TYPES[dtype]
+    data = np.frombuffer(raw, dtype=dt).copy()
+    if dtype != "int":
+        mask = np.abs(data) < 1e-30
+        data[mask] = (np.nan + 1j * np.nan) if dtype == "fcomplex" else np.nan
+    return data.astype(data.dtype.newbyteorder("="))
+
+
+def read_gamma_image(path, width: int, dtype: str = "float", y0: int = 0, ny: int | None = None) -> np.ndarray:
+    """moraine/gamma_.py:13-56 restated: lines y0 .. y0 + ny of a GAMMA raster."""
+    nb = int(GAMMA_TYPES[dtype][-1])
+    size = Path(path).stat().st_size
+    nlines = size // nb // width
+    if ny is None:
+        ny = nlines - y0
+    with open(path, "rb") as f:
+        f.seek(y0 * width * nb)
+        raw = f.read(ny * width * nb)
+    return gamma_decode(raw, dtype).reshape(-1, width)

@@ -144,14 +144,67 @@ def chain_small(mr):
                         t_coh_fused=t_f)
 
 
+def gamma_samples(rng, dtype: str, count: int) -> np.ndarray:
+    """Big-endian samples with the values the no-data rule separates (around 1e-30)."""
+    specials = [0.0, -0.0, 1e-31, -1e-31, 9.999999e-31, 1.0000001e-30, 1e-30, -1e-30, 2e-30, 1e-38, 1e-45,
+                np.inf, -np.inf, np.nan, 1.0, -3.5, 1e30]
+    if dtype == "int":
+        v = rng.integers(-2**31, 2**31 - 1, size=count, dtype=np.int64).astype(np.int32)
+        v[:5] = [0, 1, -1, 2**31 - 1, -2**31]
+        return v.astype(">i4")
+    if dtype == "fcomplex":
+        re = rng.standard_normal(count).astype(np.float32)
+        im = rng.standard_normal(count).astype(np.float32)
+        k = len(specials)
+        re[:k] = np.array(specials, np.float32)
+        im[:k] = np.array(specials[::-1], np.float32)
+        re[k:2 * k] = np.array(specials, np.float32)  # pairs with a tiny real part and a zero imaginary one
+        im[k:2 * k] = 0
+        re[2 * k:2 * k + 4] = [7e-31, 5e-31, 0, 1e-30]
+        im[2 * k:2 * k + 4] = [7e-31, 9e-31, 1e-30, 0]
+        c = np.empty(count, np.complex64)
+        c.real, c.imag = re, im
+        return c.astype(">c8")
+    f = np.float32 if dtype == "float" else np.float64
+    v = (rng.standard_normal(count) * 10).astype(f)
+    v[:len(specials)] = np.array(specials, f)
+    return v.astype(">f4" if dtype == "float" else ">f8")
+
+
+def gamma_small(src: str, rng):
+    """moraine/gamma_.py:13-56: read_gamma_image on big-endian files of every dtype."""
+    import tempfile  # noqa: PLC0415
+
+    spec = importlib.util.spec_from_file_location("moraine_gamma_ref", str(Path(src) / "moraine" / "gamma_.py"))
+    g = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(g)
+    out = {}
+    width, nlines = 13, 11
+    with tempfile.TemporaryDirectory() as td:
+        for dtype in ("float", "fcomplex", "int", "double"):
+            raw = gamma_samples(rng, dtype, width * nlines)
+            f = Path(td) / f"img.{dtype}"
+            raw.tofile(f)
+            out[f"{dtype}_raw"] = np.frombuffer(raw.tobytes(), np.uint8)
+            out[f"{dtype}_all"] = g.read_gamma_image(str(f), width, dtype)
+            out[f"{dtype}_y3_n5"] = g.read_gamma_image(str(f), width, dtype, y0=3, ny=5)
+    out["shape"] = np.array([nlines, width])
+    np.savez_compressed(HERE / "gamma_small.npz", **out)
+
+
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    src = args[0] if args else "/root/reference"
+    if "--gamma-only" in sys.argv:
+        gamma_small(src, np.random.default_rng(20240602))
+        return
     mr = load_reference(src)
     rng = np.random.default_rng(20240601)
     ks_tables(mr)
     ks_small(mr, rng)
     co_small(mr, rng)
     chain_small(mr)
+    gamma_small(src, np.random.default_rng(20240602))
     import numba  # noqa: PLC0415
 
     (HERE / "MANIFEST.txt").write_text(
