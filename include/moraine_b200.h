@@ -147,6 +147,19 @@ int mr_emperical_co(const mr_complex64* rslc, int nlines, int width, int nimages
                     const uint8_t* is_shp, int az_win, int r_win, mr_complex64* cov,
                     mr_complex64* coh, mr_stream_t stream);
 
+/* Replaces moraine.co.ad_intf_pc (moraine/co.py:376-406; GPU kernel :334-374): adaptive
+ * multilook interferogram of one pair for point-cloud data, intf = sum ref conj(sec) /
+ * sqrt(sum |ref|^2 sum |sec|^2) over each point's SHPs (pc_is_shp (n_pc, az_win, r_win)).
+ * Equal to pair (0, 1) of mr_emperical_co_pc on the stack (ref, sec, ...), as the
+ * reference's own test requires (nbs/API/co.ipynb#cell46). precision: MR_PREC_FP32
+ * (the reference GPU kernel's accumulation) or MR_PREC_FP64. workspace: >=
+ * mr_ad_intf_pc_workspace_bytes() (the two images interleaved). */
+size_t mr_ad_intf_pc_workspace_bytes(int nlines, int width);
+int mr_ad_intf_pc(const mr_complex64* ref_rslc, const mr_complex64* sec_rslc, int nlines, int width,
+                  const int32_t* idx, int64_t n_pc, const uint8_t* pc_is_shp, int az_win, int r_win,
+                  mr_complex64* intf, int precision, void* workspace, size_t workspace_bytes,
+                  mr_stream_t stream);
+
 /* Replaces moraine.co.uncompress_coh (moraine/co.py:281-299): (n, n_pairs) ->
  * (n, nimages, nimages) Hermitian, zero where no pair is given, unit diagonal. */
 int mr_uncompress_coh(const mr_complex64* coh, int64_t n, int nimages,

@@ -96,3 +96,35 @@ def uncompress_coh(coh, image_pairs=None):
     _lib.call("mr_uncompress_coh", c.data_ptr(), n, nimages, _dev.ptr(pairs), int(c.shape[-1]), out.data_ptr(),
               _dev.stream())
     return _dev.from_device(out, kind)
+
+
+def ad_intf_pc(ref_rslc, sec_rslc, idx, pc_is_shp, block_size: int = 128, precision: str = "fp32"):
+    """Adaptive multilook interferogram of one pair for point-cloud data (moraine/co.py:376-406).
+
+    ``ref_rslc``, ``sec_rslc`` (nlines, width) complex64; ``idx`` (n_pc, 2); ``pc_is_shp``
+    (n_pc, az_win, r_win) bool. Returns (n_pc,) complex64, equal to pair (0, 1) of
+    ``emperical_co_pc`` on a stack whose first two dates are ``ref_rslc`` and ``sec_rslc``.
+    ``precision`` (an addition to the reference signature): ``"fp32"`` (the reference GPU
+    kernel's accumulation) or ``"fp64"``. The reference's CPU branch cannot run (it names an
+    undefined ``rslc``, moraine/co.py:315); this one serves numpy input through the device.
+    """
+    kind = _dev.kind_of(ref_rslc)
+    dev = _dev.require_cuda()
+    a = _dev.to_device(ref_rslc, torch.complex64, dev)
+    b = _dev.to_device(sec_rslc, torch.complex64, dev)
+    if a.shape != b.shape or a.dim() != 2:
+        raise ValueError("ad_intf_pc: ref_rslc and sec_rslc must be 2-D of the same shape")
+    nlines, width = a.shape
+    ix = _dev.to_device(idx, torch.int32, dev).reshape(-1, 2)
+    m = _dev.to_device(pc_is_shp, torch.uint8, dev)
+    az_win, r_win = _window(m)
+    n_pc = ix.shape[0]
+    if m.shape[0] != n_pc:
+        raise ValueError("ad_intf_pc: idx and pc_is_shp disagree on the number of points")
+    out = torch.empty((n_pc,), dtype=torch.complex64, device=dev)
+    if n_pc:
+        lib = _lib.load()
+        ws = _dev.workspace(lib.mr_ad_intf_pc_workspace_bytes(nlines, width), dev)
+        _lib.call("mr_ad_intf_pc", a.data_ptr(), b.data_ptr(), nlines, width, ix.data_ptr(), n_pc, m.data_ptr(), az_win,
+                  r_win, out.data_ptr(), _lib.PREC[precision], ws.data_ptr(), ws.numel(), _dev.stream())
+    return _dev.from_device(out, kind)

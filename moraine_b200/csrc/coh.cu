@@ -279,6 +279,44 @@ extern "C" int mr_emperical_co_pc(const mr_complex64* rslc, int nlines, int widt
   }
 }
 
+// Two single-date images to the interleaved 2-date layout of the Gram kernels.
+__global__ void interleave2_kernel(const float2* __restrict__ a, const float2* __restrict__ b, int64_t npix,
+                                   float4* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 x = a[i], y = b[i];
+    out[i] = make_float4(x.x, x.y, y.x, y.y);
+  }
+}
+
+extern "C" size_t mr_ad_intf_pc_workspace_bytes(int nlines, int width) {
+  return std::max<size_t>(16, (size_t)nlines * width * 2 * sizeof(float2));
+}
+
+extern "C" int mr_ad_intf_pc(const mr_complex64* ref_rslc, const mr_complex64* sec_rslc, int nlines, int width,
+                             const int32_t* idx, int64_t n_pc, const uint8_t* pc_is_shp, int az_win, int r_win,
+                             mr_complex64* intf, int precision, void* workspace, size_t workspace_bytes,
+                             mr_stream_t stream) {
+  MR_REQUIRE(n_pc >= 0, "ad_intf_pc: negative n_pc");
+  if (n_pc == 0) return MR_OK;
+  MR_REQUIRE(ref_rslc && sec_rslc && idx && pc_is_shp && intf, "ad_intf_pc: NULL pointer");
+  MR_REQUIRE(nlines > 0 && width > 0, "ad_intf_pc: bad image shape");
+  MR_REQUIRE(precision == MR_PREC_FP32 || precision == MR_PREC_FP64, "ad_intf_pc: precision must be FP32 or FP64");
+  const size_t need = mr_ad_intf_pc_workspace_bytes(nlines, width);
+  if (!workspace || workspace_bytes < need)
+    return fail(MR_ERR_WORKSPACE, "ad_intf_pc: workspace %zu < %zu bytes", workspace_bytes, need);
+  MR_REQUIRE(((uintptr_t)workspace & 15) == 0, "ad_intf_pc: workspace not 16-byte aligned");
+  const int64_t npix = (int64_t)nlines * width;
+  const int grid = (int)std::min<int64_t>((npix + 255) / 256, (int64_t)sm_count() * 16);
+  interleave2_kernel<<<grid, 256, 0, as_stream(stream)>>>(reinterpret_cast<const float2*>(ref_rslc),
+                                                          reinterpret_cast<const float2*>(sec_rslc), npix,
+                                                          static_cast<float4*>(workspace));
+  if (int rc = check_launch("ad_intf_pc interleave")) return rc;
+  // the one pair (0, 1) of the 2-date stack: the same kernel and arithmetic as pair (0, 1)
+  // of emperical_co_pc on the full stack
+  return mr_emperical_co_pc(static_cast<const mr_complex64*>(workspace), nlines, width, 2, idx, n_pc, pc_is_shp, 0,
+                            az_win, r_win, nullptr, 1, intf, precision, stream);
+}
+
 extern "C" int mr_emperical_co(const mr_complex64* rslc, int nlines, int width, int nimages,
                                const uint8_t* is_shp, int az_win, int r_win, mr_complex64* cov,
                                mr_complex64* coh, mr_stream_t stream) {

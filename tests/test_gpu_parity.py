@@ -97,6 +97,22 @@ def test_co_pc_vs_oracle(cuda, name, size, precision, tol):
     assert np.abs(coh - ref).max() < tol
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_ad_intf_pc_equals_first_pair(cuda, golden, precision):
+    """The reference's own check (nbs/API/co.ipynb#cell46-47): ad_intf_pc of dates 0 and 1
+    equals pair (0, 1) of emperical_co_pc, exactly; and both agree with the oracle."""
+    g = golden("co_small.npz")
+    rslc, idx, pc = g["rslc"], g["idx"], g["pc_is_shp"]
+    coh = mb.emperical_co_pc(rslc, idx, pc, precision=precision)
+    intf = mb.ad_intf_pc(rslc[:, :, 0].copy(), rslc[:, :, 1].copy(), idx, pc, precision=precision)
+    assert intf.shape == (idx.shape[0],) and intf.dtype == np.complex64
+    np.testing.assert_array_equal(intf, coh[:, 0])
+    two = O.emperical_co_pc(rslc[:, :, :2].copy(), idx, pc)[:, 0]
+    np.testing.assert_allclose(intf, two, atol=2e-6 if precision == "fp32" else 2e-7, rtol=0)
+    with pytest.raises(ValueError):
+        mb.ad_intf_pc(rslc[:, :, 0], rslc[:-1, :, 1], idx, pc)
+
+
 def test_co_raster_vs_oracle(cuda):
     rng = np.random.default_rng(4)
     z = (rng.standard_normal((9, 13, 7)) + 1j * rng.standard_normal((9, 13, 7))).astype(np.complex64)
