@@ -166,6 +166,22 @@ int mr_uncompress_coh(const mr_complex64* coh, int64_t n, int nimages,
                       const int32_t* image_pairs, int n_pairs, mr_complex64* out,
                       mr_stream_t stream);
 
+/* ---------------------------------------------------------------- PS-side statistics */
+/* Replaces moraine.calamp.rslc2amp (moraine/calamp.py:33-41): amp = |rslc| (float32, as
+ * numpy's complex64 abs), any shape flattened to n samples. */
+int mr_rslc2amp(const mr_complex64* rslc, int64_t n, float* amp, mr_stream_t stream);
+
+/* Replaces moraine.ps.amp_disp (moraine/ps.py:65-73): per pixel of a (npix, nimages)
+ * complex64 stack, std(|z|) / mean(|z|) over the dates (population std), float32. */
+int mr_amp_disp(const mr_complex64* rslc, int64_t npix, int nimages, float* amp_disp,
+                mr_stream_t stream);
+
+/* Replaces moraine.calamp.calamp (moraine/calamp.py:63-71): amp / nanmean(amp) over the n
+ * samples of one image. workspace: >= mr_calamp_workspace_bytes(). */
+size_t mr_calamp_workspace_bytes(void);
+int mr_calamp(const float* amp, int64_t n, float* out, void* workspace, size_t workspace_bytes,
+              mr_stream_t stream);
+
 /* ---------------------------------------------------------------- GAMMA ingest
  * Sample types of GAMMA rasters (moraine/gamma_.py:24-31: float, fcomplex, int, double). */
 enum {

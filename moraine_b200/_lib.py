@@ -28,6 +28,10 @@ _SIGNATURES = {
     "mr_abi_version": (c_int, []),
     "mr_kernel_launches": (ctypes.c_uint64, []),
     "mr_gamma_sample_bytes": (c_size_t, [c_int]),
+    "mr_rslc2amp": (c_int, [P, c_int64, P, P]),
+    "mr_amp_disp": (c_int, [P, c_int64, c_int, P, P]),
+    "mr_calamp_workspace_bytes": (c_size_t, []),
+    "mr_calamp": (c_int, [P, c_int64, P, P, c_size_t, P]),
     "mr_ad_intf_pc_workspace_bytes": (c_size_t, [c_int, c_int]),
     "mr_ad_intf_pc": (c_int, [P, P, c_int, c_int, P, c_int64, P, c_int, c_int, P, c_int, P, c_size_t, P]),
     "mr_gamma_decode": (c_int, [P, c_int64, c_int, P, c_int64, P]),

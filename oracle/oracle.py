@@ -272,3 +272,29 @@ def read_gamma_image(path, width: int, dtype: str = "float", y0: int = 0, ny: in
         f.seek(y0 * width * nb)
         raw = f.read(ny * width * nb)
     return gamma_decode(raw, dtype).reshape(-1, width)
+
+
+# ----------------------------------------------------------------------------- PS-side statistics
+def rslc2amp(rslc) -> np.ndarray:
+    """moraine/calamp.py:16-23: |z| as float32, as the reference's Numba build computes it: the
+    float32 rounding of the double square root of the double sum of squares (inf if a part is)."""
+    z = np.asarray(rslc, np.complex64)
+    re, im = z.real.astype(np.float64), z.imag.astype(np.float64)
+    with np.errstate(invalid="ignore", over="ignore"):
+        a = np.sqrt(re * re + im * im).astype(np.float32)
+    a[np.isinf(re) | np.isinf(im)] = np.inf
+    return a
+
+
+def amp_disp(rslc) -> np.ndarray:
+    """moraine/ps.py:17-27: std(|z|) / mean(|z|) over the dates, in float64, stored float32."""
+    a = rslc2amp(rslc).astype(np.float64)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return (a.std(-1) / a.mean(-1)).astype(np.float32)
+
+
+def calamp(amp) -> np.ndarray:
+    """moraine/calamp.py:46-60: amp / nanmean(amp), the mean in float64."""
+    a = np.asarray(amp, np.float32)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return (a / np.float32(np.nanmean(a.astype(np.float64)))).astype(np.float32)

@@ -192,11 +192,42 @@ def gamma_small(src: str, rng):
     np.savez_compressed(HERE / "gamma_small.npz", **out)
 
 
+def ps_small(src: str, rng):
+    """moraine/ps.py:65 amp_disp and moraine/calamp.py:33,63 rslc2amp / calamp (Numba CPU path)."""
+    pkg = sys.modules.get("moraine")
+    if pkg is None or not hasattr(pkg, "utils_"):
+        load_reference(src)
+    pkg = sys.modules["moraine"]
+
+    def ld(name):
+        spec = importlib.util.spec_from_file_location(f"moraine.{name}", str(Path(src) / "moraine" / f"{name}.py"))
+        m = importlib.util.module_from_spec(spec)
+        sys.modules[f"moraine.{name}"] = m
+        spec.loader.exec_module(m)
+        return m
+
+    ps, cal = ld("ps"), ld("calamp")
+    nl, w, n = 23, 19, 17
+    z = (rng.standard_normal((nl, w, n)) + 1j * rng.standard_normal((nl, w, n))).astype(np.complex64)
+    z *= (10.0 ** rng.uniform(-1, 1, (nl, w, 1))).astype(np.float32)
+    z[0, 0, 3] = np.nan            # a NaN date
+    z[1, 1, :] = 0                 # all-zero pixel
+    z[2, 2, 5] = np.inf + 0j       # an infinite sample
+    amp = cal.rslc2amp(z)
+    amp0 = amp[:, :, 0].copy()
+    amp0[3, 4] = np.nan
+    np.savez_compressed(HERE / "ps_small.npz", rslc=z, amp=amp, amp_disp=ps.amp_disp(z), amp0=amp0,
+                        calamp=cal.calamp(amp0))
+
+
 def main():
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     src = args[0] if args else "/root/reference"
     if "--gamma-only" in sys.argv:
         gamma_small(src, np.random.default_rng(20240602))
+        return
+    if "--ps-only" in sys.argv:
+        ps_small(src, np.random.default_rng(20240603))
         return
     mr = load_reference(src)
     rng = np.random.default_rng(20240601)
@@ -205,6 +236,7 @@ def main():
     co_small(mr, rng)
     chain_small(mr)
     gamma_small(src, np.random.default_rng(20240602))
+    ps_small(src, np.random.default_rng(20240603))
     import numba  # noqa: PLC0415
 
     (HERE / "MANIFEST.txt").write_text(
