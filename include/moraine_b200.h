@@ -229,6 +229,25 @@ int mr_emi_routed(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, d
                   mr_complex64* ph, float* emi_quality, float* t_coh, uint8_t* route,
                   void* workspace, size_t workspace_bytes, mr_stream_t stream);
 
+/* ---------------------------------------------------------------- the whole chain
+ * Replaces the stage drivers moraine/cli/shp.py:33 (ks_test, select_shp), the DS selection
+ * of nbs/API/pl.ipynb#cell15, moraine/cli/co.py:33 (emperical_co_pc) and
+ * moraine/cli/pl.py:223 (emi, ds_temp_coh) for one tile in device memory:
+ * intensity -> KS test + SHP selection (window (2 az_half_win + 1) x (2 r_half_win + 1),
+ * p < p_max) -> DS points (SHP count >= min_shp, row-major order) -> per batch of at most
+ * `batch` points: coherence (gram_precision) -> EMI with temporal coherence (emi_precision:
+ * MR_PREC_FP32, MR_PREC_FP64 or MR_PREC_MIXED). Outputs for the first *n_ds points: idx
+ * (max_ds, 2), ph (max_ds, nimages), quality and t_coh (max_ds). *n_ds is a host pointer:
+ * the call synchronises `stream` once to read the DS count (fails with MR_ERR_INVALID when
+ * it exceeds max_ds). workspace: >= mr_ds_chain_workspace_bytes(), 256-byte aligned. */
+size_t mr_ds_chain_workspace_bytes(int nlines, int width, int nimages, int az_half_win,
+                                   int r_half_win, int64_t batch);
+int mr_ds_chain(const mr_complex64* rslc, int nlines, int width, int nimages, int az_half_win,
+                int r_half_win, double p_max, int min_shp, int gram_precision, int emi_precision,
+                int32_t* idx, mr_complex64* ph, float* quality, float* t_coh, int64_t max_ds,
+                int64_t* n_ds, int64_t batch, void* workspace, size_t workspace_bytes,
+                mr_stream_t stream);
+
 /* ---------------------------------------------------------------- temporal coherence
  * Replaces moraine.pl.ds_temp_coh (moraine/pl.py:126-145; kernel :104-123):
  * t = |sum_q coh_q/|coh_q| conj(ph_m) ph_j| / n_pairs. */

@@ -329,3 +329,42 @@ def test_device_chain_vs_oracle(cuda, name, size):
     assert np.all(err <= tol), (err / tol).max()
     well = tol < 1e-3
     assert np.abs(res.t_coh.cpu().numpy() - ref["t_coh"])[well].max(initial=0) < 1e-3
+
+
+@pytest.mark.parametrize("gram,emi", [("fp32", "fp32"), ("fp64", "fp64"), ("fp64", "mixed")])
+def test_ds_chain_c_abi_equals_python_chain(cuda, gram, emi):
+    """mr_ds_chain (one C call for the whole chain) gives the DsChain results bit for bit."""
+    import ctypes
+    from moraine_b200 import _dev, _lib
+    cfg = CONFIGS["c1"].scaled(nlines=72, width=64, n_patches=6)
+    z = make_stack(cfg, device=cuda)
+    ref = DsChain(72, 64, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp, precision=gram,
+                  emi_precision=emi, device=cuda).run(z)
+    lib = _lib.load()
+    npix, n, batch = 72 * 64, cfg.nimages, 1000  # several batches
+    ws = _dev.workspace(lib.mr_ds_chain_workspace_bytes(72, 64, n, cfg.az_half_win, cfg.r_half_win, batch) + 256,
+                        cuda)
+    base = (ws.data_ptr() + 255) & ~255
+    idx = torch.empty((npix, 2), dtype=torch.int32, device=cuda)
+    ph = torch.empty((npix, n), dtype=torch.complex64, device=cuda)
+    q = torch.empty((npix,), dtype=torch.float32, device=cuda)
+    t = torch.empty((npix,), dtype=torch.float32, device=cuda)
+    n_ds = ctypes.c_int64(-1)
+    args = [z.data_ptr(), 72, 64, n, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp, _lib.PREC[gram],
+            _lib.PREC[emi], idx.data_ptr(), ph.data_ptr(), q.data_ptr(), t.data_ptr(), npix, ctypes.addressof(n_ds),
+            batch, base, ws.numel() - 256, _dev.stream()]
+    _lib.call("mr_ds_chain", *args)
+    d = n_ds.value
+    assert d == ref.n_ds > batch
+    assert torch.equal(idx[:d], ref.idx)
+    assert torch.equal(ph[:d].view(torch.float32), ref.ph.view(torch.float32))
+    assert torch.equal(q[:d].view(torch.int32), ref.quality.view(torch.int32))
+    assert torch.equal(t[:d].view(torch.int32), ref.t_coh.view(torch.int32))
+    small = list(args)
+    small[14] = d - 1  # max_ds below the DS count
+    with pytest.raises(ValueError):
+        _lib.call("mr_ds_chain", *small)
+    small = list(args)
+    small[18] = 1024  # workspace too small
+    with pytest.raises(MemoryError):
+        _lib.call("mr_ds_chain", *small)
