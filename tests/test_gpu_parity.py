@@ -368,3 +368,31 @@ def test_ds_chain_c_abi_equals_python_chain(cuda, gram, emi):
     small[18] = 1024  # workspace too small
     with pytest.raises(MemoryError):
         _lib.call("mr_ds_chain", *small)
+
+
+def test_maximum_sizes(cuda):
+    """The build's limits: N = 512 images through KS (bit-exact), coherence and EMI; the
+    largest window (4096 cells) through KS; one past each limit is refused."""
+    rng = np.random.default_rng(11)
+    n = 512
+    z = (rng.standard_normal((10, 9, n)) + 1j * rng.standard_normal((10, 9, n))).astype(np.complex64)
+    z *= np.exp(1j * np.linspace(0, 3, n))[None, None, :].astype(np.complex64)
+    rmli = O.intensity(z)
+    p = mb.ks_test(rmli, 2, 2)
+    np.testing.assert_array_equal(p, O.ks_test(rmli, 2, 2))
+    idx = np.array([[4, 4], [5, 3], [2, 6]], np.int32)
+    pc = np.ones((3, 5, 5), bool)
+    coh = mb.emperical_co_pc(z, idx, pc, precision="fp64")
+    ref = O.emperical_co_pc(z, idx, pc)
+    np.testing.assert_allclose(coh, ref, atol=2e-7, rtol=0)
+    ph, q = mb.emi(coh)
+    ph_r, q_r, gap, cond = O.emi(coh)
+    err = np.abs(np.angle(ph * np.conj(ph_r))).max(-1)
+    assert np.all(err <= O.phase_tolerance(cond, gap, eps=1e3 * EPS64, floor=3e-7))
+    with pytest.raises(NotImplementedError):
+        mb.ks_test(np.ones((4, 4, n + 1), np.float32), 1, 1)
+    # largest window: 63 x 65 = 4095 cells on a small raster
+    x = rng.exponential(size=(70, 70, 9)).astype(np.float32)
+    np.testing.assert_array_equal(mb.ks_test(x, 31, 32), O.ks_test(x, 31, 32))
+    with pytest.raises(NotImplementedError):
+        mb.ks_test(x, 32, 32)  # 65 x 65 = 4225 cells
