@@ -96,7 +96,9 @@ class DsChain:
 
     def run(self, rslc: torch.Tensor) -> ChainResult:
         nlines, width, n = self.shape
-        assert rslc.shape == self.shape and rslc.dtype == torch.complex64 and rslc.is_cuda
+        if tuple(rslc.shape) != self.shape or rslc.dtype != torch.complex64 or not rslc.is_cuda:
+            raise ValueError(f"DsChain.run: expected a CUDA complex64 stack of shape {self.shape}, got "
+                             f"{rslc.dtype} {tuple(rslc.shape)} on {rslc.device}")
         rslc = rslc.contiguous()
         s = _dev.stream()
         ev = []
