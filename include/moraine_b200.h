@@ -248,6 +248,18 @@ int mr_ds_chain(const mr_complex64* rslc, int nlines, int width, int nimages, in
                 int64_t* n_ds, int64_t batch, void* workspace, size_t workspace_bytes,
                 mr_stream_t stream);
 
+/* mr_ds_chain without the host synchronisation, for capture in a CUDA graph: the DS count
+ * goes to n_ds_dev (device memory) and the kernels read it there, processing every batch
+ * that max_ds allows (batches past the count do no work). Only stream-ordered work, no
+ * allocation. Limits: nimages <= 128, gram and emi precision MR_PREC_FP32 or MR_PREC_FP64.
+ * Points past max_ds are not processed: compare *n_ds_dev with max_ds afterwards. Same
+ * results as mr_ds_chain. No reference counterpart. */
+int mr_ds_chain_async(const mr_complex64* rslc, int nlines, int width, int nimages, int az_half_win,
+                      int r_half_win, double p_max, int min_shp, int gram_precision, int emi_precision,
+                      int32_t* idx, mr_complex64* ph, float* quality, float* t_coh, int64_t max_ds,
+                      int64_t* n_ds_dev, int64_t batch, void* workspace, size_t workspace_bytes,
+                      mr_stream_t stream);
+
 /* ---------------------------------------------------------------- temporal coherence
  * Replaces moraine.pl.ds_temp_coh (moraine/pl.py:126-145; kernel :104-123):
  * t = |sum_q coh_q/|coh_q| conj(ph_m) ph_j| / n_pairs. */

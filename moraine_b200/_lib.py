@@ -31,6 +31,8 @@ _SIGNATURES = {
     "mr_ds_chain_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_int, c_int, c_int64]),
     "mr_ds_chain": (c_int, [P, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_int, c_int, P, P, P, P, c_int64, P,
                             c_int64, P, c_size_t, P]),
+    "mr_ds_chain_async": (c_int, [P, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_int, c_int, P, P, P, P,
+                                  c_int64, P, c_int64, P, c_size_t, P]),
     "mr_rslc2amp": (c_int, [P, c_int64, P, P]),
     "mr_amp_disp": (c_int, [P, c_int64, c_int, P, P]),
     "mr_calamp_workspace_bytes": (c_size_t, []),

@@ -25,8 +25,8 @@ class ChainResult:
     ph: torch.Tensor           # (n_ds, N) complex64
     quality: torch.Tensor      # (n_ds,) float32
     t_coh: torch.Tensor        # (n_ds,) float32
-    shp_num: torch.Tensor      # (nlines, width) int32
-    is_shp: torch.Tensor       # (nlines, width, az_win, r_win) uint8
+    shp_num: torch.Tensor | None  # (nlines, width) int32 (None in graph mode)
+    is_shp: torch.Tensor | None   # (nlines, width, az_win, r_win) uint8 (None in graph mode)
     stage_ms: dict = field(default_factory=dict)
     route: torch.Tensor | None = None  # (n_ds,) uint8 EMI route with emi_precision="mixed"
 
@@ -37,7 +37,7 @@ class DsChain:
     def __init__(self, nlines: int, width: int, nimages: int, az_half_win: int, r_half_win: int,
                  p_max: float = 0.05, min_shp: int = 50, precision: str = "fp32", batch: int | None = None,
                  device=None, timing: bool = False, emi_precision: str | None = None,
-                 cond_max: float = 1.0e4):
+                 cond_max: float = 1.0e4, graph: bool = False):
         self.device = torch.device(device) if device is not None else _dev.require_cuda()
         self.shape = (nlines, width, nimages)
         self.azh, self.rh = az_half_win, r_half_win
@@ -74,6 +74,19 @@ class DsChain:
         self.quality = torch.empty((npix,), dtype=torch.float32, device=d)
         self.t_coh = torch.empty((npix,), dtype=torch.float32, device=d)
         self.route = torch.empty((npix,), dtype=torch.uint8, device=d) if emi_precision == "mixed" else None
+        # CUDA-graph mode: the whole chain (mr_ds_chain_async, the DS count kept on the device)
+        # captured once and replayed for every stack copied into a static input buffer
+        self.graph = bool(graph)
+        self._graph = None
+        if self.graph:
+            if nimages > 128 or precision not in ("fp32", "fp64") or emi_precision not in ("fp32", "fp64"):
+                raise ValueError("DsChain(graph=True) needs nimages <= 128 and fp32/fp64 arithmetic")
+            self.x = torch.empty((nlines, width, nimages), dtype=torch.complex64, device=d)
+            gbytes = lib.mr_ds_chain_workspace_bytes(nlines, width, nimages, az_half_win, r_half_win, self.batch)
+            self.g_ws = _dev.workspace(gbytes + 256, d)
+            self.g_base = (self.g_ws.data_ptr() + 255) & ~255
+            self.g_bytes = gbytes
+            self.n_ds_g = torch.zeros((1,), dtype=torch.int64, device=d)
 
     @staticmethod
     def default_batch(npix: int, nimages: int) -> int:
@@ -94,12 +107,34 @@ class DsChain:
                    + lib.mr_ds_extract_workspace_bytes(npix) + npix * 8 + 8 + batch * npairs * 8
                    + lib.mr_emi_workspace_bytes(batch, nimages) + npix * nimages * 8 + npix * 8)
 
+    def _chain_async(self) -> None:
+        nlines, width, n = self.shape
+        _lib.call("mr_ds_chain_async", self.x.data_ptr(), nlines, width, n, self.azh, self.rh, self.p_max, self.min_shp,
+                  self.prec, self.emi_prec, self.idx.data_ptr(), self.ph.data_ptr(), self.quality.data_ptr(),
+                  self.t_coh.data_ptr(), nlines * width, self.n_ds_g.data_ptr(), self.batch, self.g_base,
+                  self.g_bytes, _dev.stream())
+
+    def _run_graph(self, rslc: torch.Tensor) -> ChainResult:
+        self.x.copy_(rslc)
+        if self._graph is None:
+            self._chain_async()  # first call outside the capture: kernel attributes, module load
+            torch.cuda.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._chain_async()
+            self._graph = g
+        self._graph.replay()
+        n_ds = int(self.n_ds_g.item())
+        return ChainResult(n_ds, self.idx[:n_ds], self.ph[:n_ds], self.quality[:n_ds], self.t_coh[:n_ds], None, None)
+
     def run(self, rslc: torch.Tensor) -> ChainResult:
         nlines, width, n = self.shape
         if tuple(rslc.shape) != self.shape or rslc.dtype != torch.complex64 or not rslc.is_cuda:
             raise ValueError(f"DsChain.run: expected a CUDA complex64 stack of shape {self.shape}, got "
                              f"{rslc.dtype} {tuple(rslc.shape)} on {rslc.device}")
         rslc = rslc.contiguous()
+        if self.graph:
+            return self._run_graph(rslc)
         s = _dev.stream()
         ev = []
 

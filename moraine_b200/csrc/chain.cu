@@ -4,8 +4,10 @@
 // The production caller of the kernels for hosts that bind the library directly (no
 // Python): it replaces the reference's file-based stage drivers (moraine/cli/shp.py:33,
 // moraine/cli/co.py:33, moraine/cli/pl.py:223) for one tile resident in device memory.
-// Every intermediate stays in the caller's workspace; the stream is synchronised once, to
-// read the number of DS points that sizes the batch loop.
+// Every intermediate stays in the caller's workspace. mr_ds_chain synchronises the stream
+// once, to read the number of DS points that sizes the batch loop; mr_ds_chain_async keeps
+// that count on the device (the kernels clamp to it) so that the call can be captured in a
+// CUDA graph.
 #include <algorithm>
 
 #include "common.cuh"
@@ -107,5 +109,50 @@ extern "C" int mr_ds_chain(const mr_complex64* rslc, int nlines, int width, int 
                                 w.emi_bytes, stream);
     if (rc) return rc;
   }
+  return MR_OK;
+}
+
+extern "C" int mr_ds_chain_async(const mr_complex64* rslc, int nlines, int width, int nimages, int az_half_win,
+                                 int r_half_win, double p_max, int min_shp, int gram_precision, int emi_precision,
+                                 int32_t* idx, mr_complex64* ph, float* quality, float* t_coh, int64_t max_ds,
+                                 int64_t* n_ds_dev, int64_t batch, void* workspace, size_t workspace_bytes,
+                                 mr_stream_t stream) {
+  MR_REQUIRE(rslc && idx && ph && quality && t_coh && n_ds_dev, "ds_chain_async: NULL pointer");
+  MR_REQUIRE(nlines > 0 && width > 0 && nimages >= 2, "ds_chain_async: bad stack shape");
+  MR_REQUIRE(az_half_win >= 0 && r_half_win >= 0, "ds_chain_async: negative half window");
+  MR_REQUIRE(batch > 0 && max_ds >= 0, "ds_chain_async: batch must be > 0 and max_ds >= 0");
+  if (nimages > 128)
+    return fail(MR_ERR_UNSUPPORTED, "ds_chain_async: nimages %d > 128 (use mr_ds_chain)", nimages);
+  if ((gram_precision != MR_PREC_FP32 && gram_precision != MR_PREC_FP64) ||
+      (emi_precision != MR_PREC_FP32 && emi_precision != MR_PREC_FP64))
+    return fail(MR_ERR_UNSUPPORTED, "ds_chain_async: gram and emi precision must be FP32 or FP64");
+  const int az_win = 2 * az_half_win + 1, r_win = 2 * r_half_win + 1, win = az_win * r_win;
+  const size_t need = mr_ds_chain_workspace_bytes(nlines, width, nimages, az_half_win, r_half_win, batch);
+  if (!workspace || workspace_bytes < need)
+    return fail(MR_ERR_WORKSPACE, "ds_chain_async: workspace %zu < %zu bytes", workspace_bytes, need);
+  MR_REQUIRE(((uintptr_t)workspace & 255) == 0, "ds_chain_async: workspace not 256-byte aligned");
+  const ChainWs w = layout(static_cast<unsigned char*>(workspace), nlines, width, nimages, win, batch);
+  const int64_t npix = (int64_t)nlines * width;
+  const int64_t npairs = (int64_t)nimages * (nimages - 1) / 2;
+  cudaStream_t s = as_stream(stream);
+  if (int rc = mr_intensity(rslc, npix * nimages, w.rmli, stream)) return rc;
+  if (int rc = mr_ks_test(w.rmli, nlines, width, nimages, az_half_win, r_half_win, nullptr, nullptr, p_max, w.is_shp,
+                          w.shp_num, w.ks, w.ks_bytes, stream))
+    return rc;
+  if (int rc = mr_ds_extract(w.shp_num, nullptr, nlines, width, win, min_shp, idx, nullptr, max_ds, n_ds_dev, w.ex,
+                             w.ex_bytes, stream))
+    return rc;
+  // every batch that max_ds allows; the kernels read the DS count and skip what is past it
+  for (int64_t b0 = 0; b0 < max_ds; b0 += batch) {
+    const int64_t nb = std::min<int64_t>(batch, max_ds - b0);
+    if (int rc = gram_counted(reinterpret_cast<const float2*>(rslc), nlines, width, nimages, idx + 2 * b0, nb,
+                              n_ds_dev, b0, w.is_shp, az_win, r_win, w.coh, gram_precision, s))
+      return rc;
+    if (int rc = emi_counted(w.coh, nb, n_ds_dev, b0, nimages, emi_precision,
+                             reinterpret_cast<float2*>(ph) + b0 * nimages, quality + b0, t_coh + b0, w.emi,
+                             w.emi_bytes, s))
+      return rc;
+  }
+  (void)npairs;
   return MR_OK;
 }

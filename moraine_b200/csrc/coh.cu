@@ -70,8 +70,12 @@ template <typename A, bool kFull>
 __global__ void __launch_bounds__(kGramThreads) gram_kernel(
     const float2* __restrict__ rslc, int nlines, int width, int n, const int32_t* __restrict__ idx,
     int64_t n_pc, const uint8_t* __restrict__ mask, int mask_stride, int az_win, int r_win,
-    float2* __restrict__ coh, float2* __restrict__ cov) {
+    float2* __restrict__ coh, float2* __restrict__ cov, const int64_t* __restrict__ dcount, int64_t doff) {
   using C = typename Acc2<A>::type;
+  if (dcount) {  // points doff .. doff + n_pc - 1 of a count held on the device
+    const int64_t c = *dcount - doff;
+    n_pc = c < 0 ? 0 : (c < n_pc ? c : n_pc);
+  }
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int win = az_win * r_win;
   const int npad = (n + 3) & ~3;
@@ -217,14 +221,14 @@ __global__ void gram_pairs_kernel(const float2* __restrict__ rslc, int nlines, i
 template <typename A, bool kFull>
 int launch_gram(const float2* rslc, int nlines, int width, int n, const int32_t* idx, int64_t n_pc,
                 const uint8_t* mask, int mask_stride, int az_win, int r_win, float2* coh, float2* cov,
-                cudaStream_t s) {
+                cudaStream_t s, const int64_t* dcount = nullptr, int64_t doff = 0) {
   const int npad = (n + 3) & ~3;
   const size_t smem = (size_t)kChunk * npad * sizeof(float2) + npad * sizeof(A) +
                       (size_t)az_win * r_win * sizeof(int);
   if (int rc = allow_smem(reinterpret_cast<const void*>(gram_kernel<A, kFull>), smem)) return rc;
   const int64_t grid = std::min<int64_t>(n_pc, (int64_t)sm_count() * 8);
   gram_kernel<A, kFull><<<(unsigned)grid, kGramThreads, smem, s>>>(rslc, nlines, width, n, idx, n_pc, mask,
-                                                                   mask_stride, az_win, r_win, coh, cov);
+                                                                   mask_stride, az_win, r_win, coh, cov, dcount, doff);
   return check_launch("coherence gram");
 }
 
@@ -316,6 +320,21 @@ extern "C" int mr_ad_intf_pc(const mr_complex64* ref_rslc, const mr_complex64* s
   return mr_emperical_co_pc(static_cast<const mr_complex64*>(workspace), nlines, width, 2, idx, n_pc, pc_is_shp, 0,
                             az_win, r_win, nullptr, 1, intf, precision, stream);
 }
+
+namespace mr {
+int gram_counted(const float2* rslc, int nlines, int width, int n, const int32_t* idx, int64_t n_max,
+                 const int64_t* dcount, int64_t doff, const uint8_t* mask, int az_win, int r_win, float2* coh,
+                 int precision, cudaStream_t s) {
+  if (n_max <= 0) return MR_OK;
+  if (precision == MR_PREC_FP32)
+    return launch_gram<float, false>(rslc, nlines, width, n, idx, n_max, mask, 1, az_win, r_win, coh, nullptr, s,
+                                     dcount, doff);
+  if (precision == MR_PREC_FP64)
+    return launch_gram<double, false>(rslc, nlines, width, n, idx, n_max, mask, 1, az_win, r_win, coh, nullptr, s,
+                                      dcount, doff);
+  return fail(MR_ERR_UNSUPPORTED, "device-counted coherence runs in FP32 or FP64");
+}
+}  // namespace mr
 
 extern "C" int mr_emperical_co(const mr_complex64* rslc, int nlines, int width, int nimages,
                                const uint8_t* is_shp, int az_win, int r_win, mr_complex64* cov,

@@ -49,6 +49,15 @@ int smem_optin();
 // exceed it. Safe when several host threads launch the kernel with different sizes.
 int allow_smem(const void* kernel, size_t bytes);
 
+// Work sized on the device (graph-capturable chain): the point count lives in device memory
+// (*dcount, of which points doff .. doff + n_max - 1 are this call's); the kernels clamp
+// to it, so the host launches for the largest count and never reads the real one.
+int gram_counted(const float2* rslc, int nlines, int width, int n, const int32_t* idx, int64_t n_max,
+                 const int64_t* dcount, int64_t doff, const uint8_t* mask, int az_win, int r_win, float2* coh,
+                 int precision, cudaStream_t s);
+int emi_counted(const float2* coh, int64_t n_max, const int64_t* dcount, int64_t doff, int n, int precision,
+                float2* ph, float* quality, float* tcoh, void* workspace, size_t workspace_bytes, cudaStream_t s);
+
 // Pair index of (m, j), m < j, in the row-major upper triangle of an N x N matrix
 // (the order of numpy.triu_indices(N, 1)).
 __host__ __device__ __forceinline__ int64_t triu_index(int m, int j, int n) {

@@ -34,7 +34,8 @@ namespace emi {
 int fast_supported(int n);
 size_t fast_workspace_bytes(int64_t n_pc, int n);
 int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, float cond_max, float2* ph,
-             float* quality, float* tcoh, uint8_t* route, void* workspace, cudaStream_t s);
+             float* quality, float* tcoh, uint8_t* route, void* workspace, cudaStream_t s,
+             const int64_t* dcount = nullptr, int64_t doff = 0);
 
 namespace {
 
@@ -275,3 +276,16 @@ extern "C" int mr_emi_routed(const mr_complex64* coh, int64_t n_pc, int nimages,
   return emi_entry(coh, n_pc, nimages, ref, MR_PREC_MIXED, cond_max, ph, emi_quality, t_coh, route, workspace,
                    workspace_bytes, stream);
 }
+
+namespace mr {
+int emi_counted(const float2* coh, int64_t n_max, const int64_t* dcount, int64_t doff, int n, int precision,
+                float2* ph, float* quality, float* tcoh, void* workspace, size_t workspace_bytes, cudaStream_t s) {
+  if (n_max <= 0) return MR_OK;
+  if (!emi::fast_supported(n)) return fail(MR_ERR_UNSUPPORTED, "emi: device-counted points need nimages <= 128");
+  if (precision != MR_PREC_FP32 && precision != MR_PREC_FP64)
+    return fail(MR_ERR_UNSUPPORTED, "emi: device-counted points run in FP32 or FP64");
+  if (!workspace || workspace_bytes < mr_emi_workspace_bytes(n_max, n))
+    return fail(MR_ERR_WORKSPACE, "emi: workspace too small");
+  return emi::fast_run(coh, n_max, n, 0, precision, 0.f, ph, quality, tcoh, nullptr, workspace, s, dcount, doff);
+}
+}  // namespace mr

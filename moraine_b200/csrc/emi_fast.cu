@@ -483,7 +483,16 @@ struct PointSet {
   const int32_t* list;
   const int32_t* count;
   int64_t n_pc;
-  __device__ __forceinline__ int64_t size() const { return list ? (int64_t)*count : n_pc; }
+  const int64_t* dcount;  // without a list: the points are dcount[0] - off, at most n_pc
+  int64_t off;
+  __device__ __forceinline__ int64_t size() const {
+    if (list) return (int64_t)*count;
+    if (dcount) {
+      const int64_t c = *dcount - off;
+      return c < 0 ? 0 : (c < n_pc ? c : n_pc);
+    }
+    return n_pc;
+  }
   __device__ __forceinline__ int64_t operator[](int64_t i) const { return list ? (int64_t)list[i] : i; }
 };
 
@@ -853,7 +862,10 @@ size_t fast_workspace_bytes(int64_t n_pc, int n) {
 }
 
 int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, float cond_max, float2* ph,
-             float* quality, float* tcoh, uint8_t* route, void* workspace, cudaStream_t s) {
+             float* quality, float* tcoh, uint8_t* route, void* workspace, cudaStream_t s,
+             const int64_t* dcount, int64_t doff) {
+  if (dcount && precision == MR_PREC_MIXED)
+    return fail(MR_ERR_UNSUPPORTED, "emi: device-counted points run in FP32 or FP64");
   auto* ws = static_cast<unsigned char*>(workspace);
   const bool f64 = precision == MR_PREC_FP64;
   const bool mixed = precision == MR_PREC_MIXED;
@@ -867,7 +879,7 @@ int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, flo
     float2* p = ph + b0 * n;
     float* q = quality + b0;
     float* t = tcoh ? tcoh + b0 : nullptr;
-    const PointSet all{nullptr, nullptr, nb};
+    const PointSet all{nullptr, nullptr, nb, dcount, doff + b0};
     int rc;
     if (f64) {
       rc = run_pass<double>(c, all, n, ref, p, q, t, w.pts, w.sing, 0.f, s);

@@ -396,3 +396,23 @@ def test_maximum_sizes(cuda):
     np.testing.assert_array_equal(mb.ks_test(x, 31, 32), O.ks_test(x, 31, 32))
     with pytest.raises(NotImplementedError):
         mb.ks_test(x, 32, 32)  # 65 x 65 = 4225 cells
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_chain_in_cuda_graph(cuda, prec):
+    """The chain captured once in a CUDA graph and replayed on two stacks equals the plain chain."""
+    cfg = CONFIGS["c1"].scaled(nlines=64, width=72, n_patches=6)
+    plain = DsChain(64, 72, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp, precision=prec,
+                    batch=900, device=cuda)
+    graph = DsChain(64, 72, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp, precision=prec,
+                    batch=900, device=cuda, graph=True)
+    for seed in (5, 6):
+        z = make_stack(cfg.scaled(seed=seed), device=cuda)
+        a, b = plain.run(z), graph.run(z)
+        assert b.n_ds == a.n_ds > 900
+        assert torch.equal(b.idx, a.idx)
+        assert torch.equal(b.ph.view(torch.float32), a.ph.view(torch.float32))
+        assert torch.equal(b.quality.view(torch.int32), a.quality.view(torch.int32))
+        assert torch.equal(b.t_coh.view(torch.int32), a.t_coh.view(torch.int32))
+    with pytest.raises(ValueError):
+        DsChain(8, 8, 200, 1, 1, graph=True, device=cuda)
