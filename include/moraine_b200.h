@@ -95,6 +95,15 @@ int mr_ks_test(const float* rmli, int nlines, int width, int nimages, int az_hal
 
 /* Replaces moraine.shp.select_shp (moraine/shp.py:309-323): is_shp = p < p_max (p
  * widened to double; NaN gives 0), shp_num = per-pixel count. */
+/* Tile plans of the KS merge: with autotuning on (off by default), the first mr_ks_test for a
+ * (device, nimages, window) times the plans for several shared-memory budgets on its own
+ * input (synchronising the stream; never inside a stream capture) and keeps the fastest;
+ * results do not depend on the plan. mr_ks_plan reports the plan in use. No reference
+ * counterpart (the reference kernel has no tiles). */
+void mr_set_autotune(int on);
+int mr_ks_plan(int nimages, int az_half_win, int r_half_win, int* tile_rows, int* tile_cols,
+               int* az_chunk);
+
 int mr_select_shp(const float* p, int64_t npix, int win, double p_max, uint8_t* is_shp,
                   int32_t* shp_num, mr_stream_t stream);
 

@@ -28,6 +28,8 @@ _SIGNATURES = {
     "mr_abi_version": (c_int, []),
     "mr_kernel_launches": (ctypes.c_uint64, []),
     "mr_gamma_sample_bytes": (c_size_t, [c_int]),
+    "mr_set_autotune": (None, [c_int]),
+    "mr_ks_plan": (c_int, [c_int, c_int, c_int, P, P, P]),
     "mr_ds_chain_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_int, c_int, c_int64]),
     "mr_ds_chain": (c_int, [P, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_int, c_int, P, P, P, P, c_int64, P,
                             c_int64, P, c_size_t, P]),
@@ -81,6 +83,9 @@ def load() -> ctypes.CDLL:
             fn = getattr(lib, name)
             fn.restype = res
             fn.argtypes = args
+        # tune the KS merge tiles on first use of each (device, nimages, window): one stream
+        # synchronisation, then the fastest plan; results do not depend on it
+        lib.mr_set_autotune(1)
         _lib = lib
     return _lib
 

@@ -8,7 +8,11 @@
 //   moraine/shp.py:74-76    x = (sqrt(N/2) + 0.12 + 0.11/sqrt(N/2)) * D, p stored as float32
 //   moraine/shp.py:58-72    NaN outside the image or when either pixel's last sorted value is NaN
 //   moraine/shp.py:309-323  is_shp = p < p_max (float32 p against a double p_max), count
+#include <atomic>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
@@ -231,10 +235,9 @@ void fill_table(KsTable& t, int n, double p_max) {
   }
 }
 
-KsPlan plan_ks(int n, int azh, int rh) {
+KsPlan plan_ks(int n, int azh, int rh, size_t budget = 200 * 1024) {
   const int az_win = 2 * azh + 1;
   KsPlan best{0, 0, 0, (n + 1) | 1, 0};
-  const size_t budget = 200 * 1024;
   double best_score = -1;
   const int tws[] = {32, 16, 8, 4, 2, 1};
   for (int tw : tws) {
@@ -303,6 +306,100 @@ extern "C" size_t mr_ks_workspace_bytes(int nlines, int width, int nimages) {
   return (size_t)nlines * width * key_stride(nimages) * sizeof(uint32_t);
 }
 
+namespace mr {
+namespace {
+
+// Autotuned merge plans: the heuristic plans for several shared-memory budgets (large
+// tiles with one CTA per SM down to small tiles with several) are timed on the first call
+// for a (device, N, window) and the fastest is kept. Every plan gives the same results.
+std::atomic<int> g_autotune{0};
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, KsPlan> g_tuned;
+
+std::vector<KsPlan> plan_candidates(int n, int azh, int rh) {
+  std::vector<KsPlan> out;
+  for (size_t budget : {200u * 1024u, 100u * 1024u, 64u * 1024u, 40u * 1024u}) {
+    const KsPlan c = plan_ks(n, azh, rh, budget);
+    if (c.th == 0) continue;
+    bool dup = false;
+    for (const KsPlan& o : out) dup |= (o.th == c.th && o.tw == c.tw && o.azc == c.azc);
+    if (!dup) out.push_back(c);
+  }
+  return out;
+}
+
+int launch_merge(const KsPlan& plan, const uint32_t* keys, int nlines, int width, int n, int azh, int rh,
+                 const KsTable& tab, float* p, float* dist, uint8_t* is_shp, int32_t* shp_num, cudaStream_t s) {
+  if (int rc = allow_smem(reinterpret_cast<const void*>(ks_merge_kernel), plan.smem)) return rc;
+  const int64_t tiles = (int64_t)((nlines + plan.th - 1) / plan.th) * ((width + plan.tw - 1) / plan.tw);
+  MR_REQUIRE(tiles < (1ll << 31), "ks_test: image too large");
+  ks_merge_kernel<<<(unsigned)tiles, kKsThreads, plan.smem, s>>>(keys, nlines, width, n, azh, rh, plan.th, plan.tw,
+                                                                 plan.azc, plan.ss, tab, p, dist, is_shp, shp_num);
+  return check_launch("ks_test merge");
+}
+
+// The plan for this call: tuned when asked and possible (never inside a stream capture).
+int choose_plan(KsPlan& plan, const uint32_t* keys, int nlines, int width, int n, int azh, int rh,
+                const KsTable& tab, float* p, float* dist, uint8_t* is_shp, int32_t* shp_num, cudaStream_t s) {
+  plan = plan_ks(n, azh, rh);
+  if (!g_autotune.load() || plan.th == 0) return MR_OK;
+  int dev = 0;
+  MR_CUDA_TRY(cudaGetDevice(&dev));
+  const auto key = std::make_tuple(dev, n, azh, rh);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) { plan = it->second; return MR_OK; }
+  }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  MR_CUDA_TRY(cudaStreamIsCapturing(s, &cap));
+  if (cap != cudaStreamCaptureStatusNone) return MR_OK;
+  cudaEvent_t e0, e1;
+  MR_CUDA_TRY(cudaEventCreate(&e0));
+  MR_CUDA_TRY(cudaEventCreate(&e1));
+  float best = 0.f;
+  KsPlan pick = plan;
+  int rc = MR_OK;
+  for (const KsPlan& c : plan_candidates(n, azh, rh)) {
+    if ((rc = launch_merge(c, keys, nlines, width, n, azh, rh, tab, p, dist, is_shp, shp_num, s))) break;  // warm
+    cudaEventRecord(e0, s);
+    if ((rc = launch_merge(c, keys, nlines, width, n, azh, rh, tab, p, dist, is_shp, shp_num, s))) break;
+    cudaEventRecord(e1, s);
+    if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(MR_ERR_CUDA, "ks_test: autotune timing failed"); break; }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (best == 0.f || ms < best) { best = ms; pick = c; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  plan = pick;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tuned[key] = pick;
+  return MR_OK;
+}
+
+}  // namespace
+}  // namespace mr
+
+extern "C" void mr_set_autotune(int on) { mr::g_autotune.store(on ? 1 : 0); }
+
+extern "C" int mr_ks_plan(int nimages, int az_half_win, int r_half_win, int* tile_rows, int* tile_cols,
+                          int* az_chunk) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  mr::KsPlan plan = mr::plan_ks(nimages, az_half_win, r_half_win);
+  {
+    std::lock_guard<std::mutex> lk(mr::g_tune_mu);
+    auto it = mr::g_tuned.find(std::make_tuple(dev, nimages, az_half_win, r_half_win));
+    if (it != mr::g_tuned.end()) plan = it->second;
+  }
+  if (tile_rows) *tile_rows = plan.th;
+  if (tile_cols) *tile_cols = plan.tw;
+  if (az_chunk) *az_chunk = plan.azc;
+  return plan.th == 0 ? MR_ERR_UNSUPPORTED : MR_OK;
+}
+
 extern "C" int mr_ks_test(const float* rmli, int nlines, int width, int nimages, int az_half_win,
                           int r_half_win, float* p, float* dist, double p_max, uint8_t* is_shp,
                           int32_t* shp_num, void* workspace, size_t workspace_bytes,
@@ -331,20 +428,18 @@ extern "C" int mr_ks_test(const float* rmli, int nlines, int width, int nimages,
   if (int rc = check_launch("ks_test sort")) return rc;
   if (!p && !dist && !is_shp) return MR_OK;
 
-  KsPlan plan = plan_ks(nimages, az_half_win, r_half_win);
-  if (plan.th == 0)
-    return fail(MR_ERR_UNSUPPORTED, "ks_test: nimages %d with half windows (%d, %d) does not fit shared memory",
-                nimages, az_half_win, r_half_win);
   // host staging of the table; the launch copies it into the kernel's parameter buffer
   static thread_local KsTable tab_local;
   fill_table(tab_local, nimages, p_max);
-  if (int rc_ = allow_smem(reinterpret_cast<const void*>(ks_merge_kernel), (size_t)(plan.smem))) return rc_;
-  const int64_t tiles = (int64_t)((nlines + plan.th - 1) / plan.th) * ((width + plan.tw - 1) / plan.tw);
-  MR_REQUIRE(tiles < (1ll << 31), "ks_test: image too large");
-  ks_merge_kernel<<<(unsigned)tiles, kKsThreads, plan.smem, s>>>(
-      keys, nlines, width, nimages, az_half_win, r_half_win, plan.th, plan.tw, plan.azc, plan.ss,
-      tab_local, p, dist, is_shp, shp_num);
-  return check_launch("ks_test merge");
+  KsPlan plan;
+  if (int rc = choose_plan(plan, keys, nlines, width, nimages, az_half_win, r_half_win, tab_local, p, dist, is_shp,
+                           shp_num, s))
+    return rc;
+  if (plan.th == 0)
+    return fail(MR_ERR_UNSUPPORTED, "ks_test: nimages %d with half windows (%d, %d) does not fit shared memory",
+                nimages, az_half_win, r_half_win);
+  return launch_merge(plan, keys, nlines, width, nimages, az_half_win, r_half_win, tab_local, p, dist, is_shp,
+                      shp_num, s);
 }
 
 extern "C" int mr_select_shp(const float* p, int64_t npix, int win, double p_max, uint8_t* is_shp,

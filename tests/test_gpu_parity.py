@@ -416,3 +416,26 @@ def test_chain_in_cuda_graph(cuda, prec):
         assert torch.equal(b.t_coh.view(torch.int32), a.t_coh.view(torch.int32))
     with pytest.raises(ValueError):
         DsChain(8, 8, 200, 1, 1, graph=True, device=cuda)
+
+
+def test_ks_autotune_same_results(cuda):
+    """Tuned and heuristic KS tile plans give bit-identical p, masks and counts."""
+    import ctypes
+    from moraine_b200 import _lib
+    lib = _lib.load()
+    cfg = CONFIGS["c1"].scaled(nlines=90, width=70)
+    z = make_stack(cfg)
+    rmli = torch.from_numpy(O.intensity(z.numpy())).to(cuda)
+    out = []
+    try:
+        for tune in (0, 1):
+            lib.mr_set_autotune(tune)
+            out.append(_fused_select(rmli, cfg.az_half_win, cfg.r_half_win))
+        th, tw, azc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        assert lib.mr_ks_plan(cfg.nimages, cfg.az_half_win, cfg.r_half_win, ctypes.byref(th), ctypes.byref(tw),
+                              ctypes.byref(azc)) == 0
+        assert th.value * tw.value >= 1 and 1 <= azc.value <= cfg.az_win
+    finally:
+        lib.mr_set_autotune(1)
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
