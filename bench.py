@@ -519,7 +519,8 @@ def main():
 
     # precision variants on the same stack, against the headline's FP64 chain
     variants = None
-    if not args.no_variants and rank == 0 and args.precision == "fp64" and chain.emi_precision == "fp64":
+    # single-GPU reports (precision variants, serving): only at N = 1, so that ranks stay in step
+    if not args.no_variants and world == 1 and args.precision == "fp64" and chain.emi_precision == "fp64":
         variants = precision_variants(cfg, rslc, res, dev)
 
     # rooflines: every stage against its bound; the headline is the dominant stage
@@ -532,7 +533,7 @@ def main():
     if roofline:
         roofline["stage"] = dom
     latency = None
-    if args.serve_requests > 0:
+    if args.serve_requests > 0 and world == 1:
         log(f"serving episode: {args.serve_requests} tiles")
         latency = serving_episode(dev, args)
         log(f"serving: p50 {latency['p50_ms']:.1f} ms, p99 {latency['p99_ms']:.1f} ms")
