@@ -106,7 +106,7 @@ __device__ __forceinline__ void load_abs_gamma(T (&a)[NB][GjGrid<NB, CX>::NC], u
 }
 
 __device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
-__device__ __forceinline__ double recip(double x) { return 1.0 / x; }
+__device__ __forceinline__ double recip(double x) { return __drcp_rn(x); }  // = 1.0 / x, IEEE round-to-nearest
 
 // One Gauss-Jordan step k = CX KB + kt on the register tile; KB is a compile-time column
 // slot, so the pivot column is read and rewritten without dynamic register indexing.

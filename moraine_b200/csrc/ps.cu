@@ -7,8 +7,8 @@
 //
 // |z| is the float32 rounding of the double square root of the exact double sum of squares,
 // +inf when either part is infinite: bit-exact with np.abs on complex64 in the reference's
-// Numba build (numpy's own hypotf can differ in the last bit). Means and standard deviations accumulate in double and the
-// ratio rounds once to float32.
+// Numba build (numpy's own hypotf can differ in the last bit). Means and standard
+// deviations accumulate in double and the ratio rounds once to float32.
 #include <algorithm>
 
 #include "common.cuh"
