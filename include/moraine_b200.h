@@ -56,6 +56,13 @@ enum {
                          the threshold (or that are singular in FP32) redone in FP64 */
 };
 
+/* What the whole chain feeds the KS test (the test depends only on ranks, but the two
+ * roundings make different ties, so the mask follows the choice bit for bit). */
+enum {
+  MR_KS_INTENSITY = 0, /* |z|^2 (mr_intensity): the rmli of the reference's API notebooks */
+  MR_KS_AMPLITUDE = 1, /* |z| (mr_rslc2amp): moraine/cli/shp.py:98, rslc2amp before ks_test */
+};
+
 /* Condition threshold of MR_PREC_MIXED in mr_emi. */
 #define MR_EMI_COND_MAX 1.0e4
 
@@ -242,9 +249,9 @@ int mr_emi_routed(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, d
  * Replaces the stage drivers moraine/cli/shp.py:33 (ks_test, select_shp), the DS selection
  * of nbs/API/pl.ipynb#cell15, moraine/cli/co.py:33 (emperical_co_pc) and
  * moraine/cli/pl.py:223 (emi, ds_temp_coh) for one tile in device memory:
- * intensity -> KS test + SHP selection (window (2 az_half_win + 1) x (2 r_half_win + 1),
- * p < p_max) -> DS points (SHP count >= min_shp, row-major order) -> per batch of at most
- * `batch` points: coherence (gram_precision) -> EMI with temporal coherence (emi_precision:
+ * KS input (ks_input: MR_KS_INTENSITY or MR_KS_AMPLITUDE) -> KS test + SHP selection
+ * (window (2 az_half_win + 1) x (2 r_half_win + 1), p < p_max) -> DS points (SHP count
+ * >= min_shp, row-major order) -> per batch of at most `batch` points: coherence (gram_precision) -> EMI with temporal coherence (emi_precision:
  * MR_PREC_FP32, MR_PREC_FP64 or MR_PREC_MIXED). Outputs for the first *n_ds points: idx
  * (max_ds, 2), ph (max_ds, nimages), quality and t_coh (max_ds). *n_ds is a host pointer:
  * the call synchronises `stream` once to read the DS count (fails with MR_ERR_INVALID when
@@ -252,8 +259,8 @@ int mr_emi_routed(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, d
 size_t mr_ds_chain_workspace_bytes(int nlines, int width, int nimages, int az_half_win,
                                    int r_half_win, int64_t batch);
 int mr_ds_chain(const mr_complex64* rslc, int nlines, int width, int nimages, int az_half_win,
-                int r_half_win, double p_max, int min_shp, int gram_precision, int emi_precision,
-                int32_t* idx, mr_complex64* ph, float* quality, float* t_coh, int64_t max_ds,
+                int r_half_win, int ks_input, double p_max, int min_shp, int gram_precision,
+                int emi_precision, int32_t* idx, mr_complex64* ph, float* quality, float* t_coh, int64_t max_ds,
                 int64_t* n_ds, int64_t batch, void* workspace, size_t workspace_bytes,
                 mr_stream_t stream);
 
@@ -264,8 +271,8 @@ int mr_ds_chain(const mr_complex64* rslc, int nlines, int width, int nimages, in
  * Points past max_ds are not processed: compare *n_ds_dev with max_ds afterwards. Same
  * results as mr_ds_chain. No reference counterpart. */
 int mr_ds_chain_async(const mr_complex64* rslc, int nlines, int width, int nimages, int az_half_win,
-                      int r_half_win, double p_max, int min_shp, int gram_precision, int emi_precision,
-                      int32_t* idx, mr_complex64* ph, float* quality, float* t_coh, int64_t max_ds,
+                      int r_half_win, int ks_input, double p_max, int min_shp, int gram_precision,
+                      int emi_precision, int32_t* idx, mr_complex64* ph, float* quality, float* t_coh, int64_t max_ds,
                       int64_t* n_ds_dev, int64_t batch, void* workspace, size_t workspace_bytes,
                       mr_stream_t stream);
 

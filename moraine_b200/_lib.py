@@ -18,6 +18,7 @@ MR_ERR_UNSUPPORTED = -3
 MR_ERR_WORKSPACE = -4
 
 PREC = {"fp32": 0, "bf16": 1, "bf16x3": 2, "fp64": 3, "mixed": 4}
+KS_INPUT = {"intensity": 0, "amplitude": 1}
 
 MAX_NIMAGES = 512
 MAX_WINDOW = 4096
@@ -31,10 +32,10 @@ _SIGNATURES = {
     "mr_set_autotune": (None, [c_int]),
     "mr_ks_plan": (c_int, [c_int, c_int, c_int, P, P, P]),
     "mr_ds_chain_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_int, c_int, c_int64]),
-    "mr_ds_chain": (c_int, [P, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_int, c_int, P, P, P, P, c_int64, P,
-                            c_int64, P, c_size_t, P]),
-    "mr_ds_chain_async": (c_int, [P, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_int, c_int, P, P, P, P,
-                                  c_int64, P, c_int64, P, c_size_t, P]),
+    "mr_ds_chain": (c_int, [P, c_int, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_int, c_int, P, P, P, P,
+                            c_int64, P, c_int64, P, c_size_t, P]),
+    "mr_ds_chain_async": (c_int, [P, c_int, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_int, c_int, P, P, P,
+                                  P, c_int64, P, c_int64, P, c_size_t, P]),
     "mr_rslc2amp": (c_int, [P, c_int64, P, P]),
     "mr_amp_disp": (c_int, [P, c_int64, c_int, P, P]),
     "mr_calamp_workspace_bytes": (c_size_t, []),

@@ -3,11 +3,17 @@
 Replaces the reference's file-based stage drivers (moraine/cli/shp.py:33-123,
 moraine/cli/co.py:33-157, moraine/cli/pl.py:223-361) for one tile resident in HBM:
 
-    rslc -> intensity -> KS test + selection -> DS candidates
+    rslc -> |z|^2 or |z| -> KS test + selection -> DS candidates
          -> [coherence -> EMI (+ temporal coherence)] per batch of DS points
 
 Every intermediate (intensity, sort keys, SHP masks, counts, DS indices, coherence of
 the current batch) stays on the device; buffers are allocated once per plan and reused.
+
+``ks_input`` chooses what the KS test ranks: ``"intensity"`` (|z|^2, the rmli of the
+reference's API notebooks and of the benchmark scene) or ``"amplitude"`` (|z| as
+``rslc2amp`` computes it, the input of the reference's CLI, moraine/cli/shp.py:98). The
+test depends only on ranks, but the two roundings make different ties, so each choice is
+bit-exact with the reference only against its own input.
 """
 from __future__ import annotations
 
@@ -37,8 +43,11 @@ class DsChain:
     def __init__(self, nlines: int, width: int, nimages: int, az_half_win: int, r_half_win: int,
                  p_max: float = 0.05, min_shp: int = 50, precision: str = "fp32", batch: int | None = None,
                  device=None, timing: bool = False, emi_precision: str | None = None,
-                 cond_max: float = 1.0e4, graph: bool = False):
+                 cond_max: float = 1.0e4, graph: bool = False, ks_input: str = "intensity"):
         self.device = torch.device(device) if device is not None else _dev.require_cuda()
+        if ks_input not in _lib.KS_INPUT:
+            raise ValueError(f"ks_input must be 'intensity' or 'amplitude', not {ks_input!r}")
+        self.ks_input = ks_input
         self.shape = (nlines, width, nimages)
         self.azh, self.rh = az_half_win, r_half_win
         self.az_win, self.r_win = 2 * az_half_win + 1, 2 * r_half_win + 1
@@ -109,9 +118,9 @@ class DsChain:
 
     def _chain_async(self) -> None:
         nlines, width, n = self.shape
-        _lib.call("mr_ds_chain_async", self.x.data_ptr(), nlines, width, n, self.azh, self.rh, self.p_max, self.min_shp,
-                  self.prec, self.emi_prec, self.idx.data_ptr(), self.ph.data_ptr(), self.quality.data_ptr(),
-                  self.t_coh.data_ptr(), nlines * width, self.n_ds_g.data_ptr(), self.batch, self.g_base,
+        _lib.call("mr_ds_chain_async", self.x.data_ptr(), nlines, width, n, self.azh, self.rh,
+                  _lib.KS_INPUT[self.ks_input], self.p_max, self.min_shp, self.prec, self.emi_prec,
+                  self.idx.data_ptr(), self.ph.data_ptr(), self.quality.data_ptr(), self.t_coh.data_ptr(), nlines * width, self.n_ds_g.data_ptr(), self.batch, self.g_base,
                   self.g_bytes, _dev.stream())
 
     def _run_graph(self, rslc: torch.Tensor) -> ChainResult:
@@ -145,7 +154,8 @@ class DsChain:
                 ev.append((name, e))
 
         mark("start")
-        _lib.call("mr_intensity", rslc.data_ptr(), rslc.numel(), self.rmli.data_ptr(), s)
+        prologue = "mr_intensity" if self.ks_input == "intensity" else "mr_rslc2amp"
+        _lib.call(prologue, rslc.data_ptr(), rslc.numel(), self.rmli.data_ptr(), s)
         mark("intensity")
         _lib.call("mr_ks_test", self.rmli.data_ptr(), nlines, width, n, self.azh, self.rh, None, None, self.p_max,
                   self.is_shp.data_ptr(), self.shp_num.data_ptr(), self.ks_ws.data_ptr(), self.ks_ws.numel(), s)

@@ -1,4 +1,4 @@
-// The whole DS chain behind one C-ABI call: intensity -> KS test + SHP selection -> DS
+// The whole DS chain behind one C-ABI call: intensity or amplitude -> KS test + SHP selection -> DS
 // extraction -> [coherence -> EMI + temporal coherence] per batch of DS points.
 //
 // The production caller of the kernels for hosts that bind the library directly (no
@@ -49,6 +49,13 @@ ChainWs layout(unsigned char* base, int nlines, int width, int n, int win, int64
   return w;
 }
 
+// The rmli the KS test reads: |z|^2 (the API notebooks) or |z| (the CLI's rslc2amp).
+int ks_prologue(const mr_complex64* rslc, int64_t n, int ks_input, float* rmli, mr_stream_t stream) {
+  if (ks_input == MR_KS_INTENSITY) return mr_intensity(rslc, n, rmli, stream);
+  if (ks_input == MR_KS_AMPLITUDE) return mr_rslc2amp(rslc, n, rmli, stream);
+  return fail(MR_ERR_INVALID, "ds_chain: ks_input %d is neither MR_KS_INTENSITY nor MR_KS_AMPLITUDE", ks_input);
+}
+
 }  // namespace
 }  // namespace mr
 
@@ -62,9 +69,9 @@ extern "C" size_t mr_ds_chain_workspace_bytes(int nlines, int width, int nimages
 }
 
 extern "C" int mr_ds_chain(const mr_complex64* rslc, int nlines, int width, int nimages, int az_half_win,
-                           int r_half_win, double p_max, int min_shp, int gram_precision, int emi_precision,
-                           int32_t* idx, mr_complex64* ph, float* quality, float* t_coh, int64_t max_ds,
-                           int64_t* n_ds, int64_t batch, void* workspace, size_t workspace_bytes,
+                           int r_half_win, int ks_input, double p_max, int min_shp, int gram_precision,
+                           int emi_precision, int32_t* idx, mr_complex64* ph, float* quality, float* t_coh,
+                           int64_t max_ds, int64_t* n_ds, int64_t batch, void* workspace, size_t workspace_bytes,
                            mr_stream_t stream) {
   MR_REQUIRE(rslc && idx && ph && quality && t_coh && n_ds, "ds_chain: NULL pointer");
   MR_REQUIRE(nlines > 0 && width > 0 && nimages >= 2, "ds_chain: bad stack shape");
@@ -82,7 +89,7 @@ extern "C" int mr_ds_chain(const mr_complex64* rslc, int nlines, int width, int 
   const int64_t npairs = (int64_t)nimages * (nimages - 1) / 2;
   cudaStream_t s = as_stream(stream);
   *n_ds = 0;
-  if (int rc = mr_intensity(rslc, npix * nimages, w.rmli, stream)) return rc;
+  if (int rc = ks_prologue(rslc, npix * nimages, ks_input, w.rmli, stream)) return rc;
   if (int rc = mr_ks_test(w.rmli, nlines, width, nimages, az_half_win, r_half_win, nullptr, nullptr, p_max, w.is_shp,
                           w.shp_num, w.ks, w.ks_bytes, stream))
     return rc;
@@ -113,10 +120,10 @@ extern "C" int mr_ds_chain(const mr_complex64* rslc, int nlines, int width, int 
 }
 
 extern "C" int mr_ds_chain_async(const mr_complex64* rslc, int nlines, int width, int nimages, int az_half_win,
-                                 int r_half_win, double p_max, int min_shp, int gram_precision, int emi_precision,
-                                 int32_t* idx, mr_complex64* ph, float* quality, float* t_coh, int64_t max_ds,
-                                 int64_t* n_ds_dev, int64_t batch, void* workspace, size_t workspace_bytes,
-                                 mr_stream_t stream) {
+                                 int r_half_win, int ks_input, double p_max, int min_shp, int gram_precision,
+                                 int emi_precision, int32_t* idx, mr_complex64* ph, float* quality, float* t_coh,
+                                 int64_t max_ds, int64_t* n_ds_dev, int64_t batch, void* workspace,
+                                 size_t workspace_bytes, mr_stream_t stream) {
   MR_REQUIRE(rslc && idx && ph && quality && t_coh && n_ds_dev, "ds_chain_async: NULL pointer");
   MR_REQUIRE(nlines > 0 && width > 0 && nimages >= 2, "ds_chain_async: bad stack shape");
   MR_REQUIRE(az_half_win >= 0 && r_half_win >= 0, "ds_chain_async: negative half window");
@@ -135,7 +142,7 @@ extern "C" int mr_ds_chain_async(const mr_complex64* rslc, int nlines, int width
   const int64_t npix = (int64_t)nlines * width;
   const int64_t npairs = (int64_t)nimages * (nimages - 1) / 2;
   cudaStream_t s = as_stream(stream);
-  if (int rc = mr_intensity(rslc, npix * nimages, w.rmli, stream)) return rc;
+  if (int rc = ks_prologue(rslc, npix * nimages, ks_input, w.rmli, stream)) return rc;
   if (int rc = mr_ks_test(w.rmli, nlines, width, nimages, az_half_win, r_half_win, nullptr, nullptr, p_max, w.is_shp,
                           w.shp_num, w.ks, w.ks_bytes, stream))
     return rc;

@@ -234,9 +234,13 @@ def intensity(rslc: np.ndarray) -> np.ndarray:
     return (re * re) + (im * im)
 
 
-def chain(rslc, az_half_win, r_half_win, p_max=0.05, min_shp=50, nthreads: int = 0, emi_chunk: int = 4096):
-    """KS -> select -> DS candidates -> coherence -> EMI -> temporal coherence, on the host."""
-    rmli = intensity(rslc)
+def chain(rslc, az_half_win, r_half_win, p_max=0.05, min_shp=50, nthreads: int = 0, emi_chunk: int = 4096,
+          ks_input: str = "intensity"):
+    """KS -> select -> DS candidates -> coherence -> EMI -> temporal coherence, on the host.
+
+    ks_input: "intensity" ranks |z|^2 (the API notebooks, nbs/API/pl.ipynb cell 15) and
+    "amplitude" ranks |z| (the CLI, rslc2amp before ks_test, moraine/cli/shp.py:98)."""
+    rmli = intensity(rslc) if ks_input == "intensity" else rslc2amp(rslc)
     p = ks_test(rmli, az_half_win, r_half_win, nthreads=nthreads)
     is_shp, shp_num = select_shp(p, p_max)
     idx, pc = ds_candidates(is_shp, shp_num, min_shp)

@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_version_and_sizes():
     lib = _lib.load()
-    assert lib.mr_abi_version() == 1
+    assert lib.mr_abi_version() == 2
     assert lib.mr_ks_workspace_bytes(200, 200, 17) == 200 * 200 * 20 * 4
     assert lib.mr_ks_workspace_bytes(0, 200, 17) == 0
     assert lib.mr_ds_extract_workspace_bytes(4096) == 4 * 8

@@ -331,15 +331,38 @@ def test_device_chain_vs_oracle(cuda, name, size):
     assert np.abs(res.t_coh.cpu().numpy() - ref["t_coh"])[well].max(initial=0) < 1e-3
 
 
-@pytest.mark.parametrize("gram,emi", [("fp32", "fp32"), ("fp64", "fp64"), ("fp64", "mixed")])
-def test_ds_chain_c_abi_equals_python_chain(cuda, gram, emi):
+@pytest.mark.parametrize("ks_input", ["intensity", "amplitude"])
+def test_chain_ks_input_vs_oracle(cuda, ks_input):
+    """The chain ranks |z|^2 or |z| as asked: SHP mask, counts and DS points bit-exact with the
+    oracle chain on the same KS input, and the amplitude mask equal to ks_test on rslc2amp."""
+    cfg = CONFIGS["c1"].scaled(nlines=80, width=80)
+    z = make_stack(cfg)
+    # range neighbours share four dates up to a phase rotation: |z| ties more often than |z|^2
+    z[:, 1::2, :4] = z[:, 0:-1:2, :4] * torch.tensor(np.exp(0.7j), dtype=torch.complex64)
+    ref = O.chain(z.numpy(), cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp, ks_input=ks_input)
+    res = DsChain(80, 80, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp, batch=4096,
+                  ks_input=ks_input).run(z.to(cuda))
+    np.testing.assert_array_equal(res.is_shp.cpu().numpy().astype(bool), ref["is_shp"])
+    np.testing.assert_array_equal(res.shp_num.cpu().numpy(), ref["shp_num"])
+    np.testing.assert_array_equal(res.idx.cpu().numpy(), ref["idx"])
+    if ks_input == "amplitude":
+        p = mb.ks_test(mb.rslc2amp(z.to(cuda)), cfg.az_half_win, cfg.r_half_win)
+        is_shp, shp_num = mb.select_shp(p, cfg.p_max)
+        assert torch.equal(is_shp.to(torch.uint8), res.is_shp) and torch.equal(shp_num.to(torch.int32), res.shp_num)
+    with pytest.raises(ValueError):
+        DsChain(8, 8, 10, 1, 1, ks_input="power", device=cuda)
+
+
+@pytest.mark.parametrize("gram,emi,ks_input", [("fp32", "fp32", "intensity"), ("fp64", "fp64", "intensity"),
+                                               ("fp64", "mixed", "intensity"), ("fp64", "fp64", "amplitude")])
+def test_ds_chain_c_abi_equals_python_chain(cuda, gram, emi, ks_input):
     """mr_ds_chain (one C call for the whole chain) gives the DsChain results bit for bit."""
     import ctypes
     from moraine_b200 import _dev, _lib
     cfg = CONFIGS["c1"].scaled(nlines=72, width=64, n_patches=6)
     z = make_stack(cfg, device=cuda)
     ref = DsChain(72, 64, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp, precision=gram,
-                  emi_precision=emi, device=cuda).run(z)
+                  emi_precision=emi, device=cuda, ks_input=ks_input).run(z)
     lib = _lib.load()
     npix, n, batch = 72 * 64, cfg.nimages, 1000  # several batches
     ws = _dev.workspace(lib.mr_ds_chain_workspace_bytes(72, 64, n, cfg.az_half_win, cfg.r_half_win, batch) + 256,
@@ -350,7 +373,8 @@ def test_ds_chain_c_abi_equals_python_chain(cuda, gram, emi):
     q = torch.empty((npix,), dtype=torch.float32, device=cuda)
     t = torch.empty((npix,), dtype=torch.float32, device=cuda)
     n_ds = ctypes.c_int64(-1)
-    args = [z.data_ptr(), 72, 64, n, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp, _lib.PREC[gram],
+    args = [z.data_ptr(), 72, 64, n, cfg.az_half_win, cfg.r_half_win, _lib.KS_INPUT[ks_input], cfg.p_max,
+            cfg.min_shp, _lib.PREC[gram],
             _lib.PREC[emi], idx.data_ptr(), ph.data_ptr(), q.data_ptr(), t.data_ptr(), npix, ctypes.addressof(n_ds),
             batch, base, ws.numel() - 256, _dev.stream()]
     _lib.call("mr_ds_chain", *args)
@@ -361,12 +385,16 @@ def test_ds_chain_c_abi_equals_python_chain(cuda, gram, emi):
     assert torch.equal(q[:d].view(torch.int32), ref.quality.view(torch.int32))
     assert torch.equal(t[:d].view(torch.int32), ref.t_coh.view(torch.int32))
     small = list(args)
-    small[14] = d - 1  # max_ds below the DS count
+    small[15] = d - 1  # max_ds below the DS count
     with pytest.raises(ValueError):
         _lib.call("mr_ds_chain", *small)
     small = list(args)
-    small[18] = 1024  # workspace too small
+    small[19] = 1024  # workspace too small
     with pytest.raises(MemoryError):
+        _lib.call("mr_ds_chain", *small)
+    small = list(args)
+    small[6] = 2  # neither intensity nor amplitude
+    with pytest.raises(ValueError):
         _lib.call("mr_ds_chain", *small)
 
 

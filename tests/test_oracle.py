@@ -150,3 +150,19 @@ def test_chain_small_matches_reference(golden):
     # reference fused helper == separate calls (nbs/API/pl.ipynb cell 38)
     np.testing.assert_array_equal(g["ph"], g["ph_fused"])
     np.testing.assert_array_equal(g["t_coh"], g["t_coh_fused"])
+
+
+def test_ks_input_choice_changes_ties():
+    """|z| and |z|^2 rank near-tied samples differently, so the KS input of a chain is part of
+    its result: the CLI's rslc2amp (moraine/cli/shp.py:98) and the notebooks' |z|^2 give
+    different p values on samples whose magnitudes agree to rounding."""
+    rng = np.random.default_rng(11)
+    z = (rng.standard_normal((24, 24, 30)) + 1j * rng.standard_normal((24, 24, 30))).astype(np.complex64)
+    # range neighbours share four dates up to a phase rotation: equal magnitudes, different roundings
+    z[:, 1::2, :4] = z[:, 0:-1:2, :4] * np.complex64(np.exp(0.7j))
+    amp, inten = O.rslc2amp(z), O.intensity(z)
+    assert (amp[:, 1::2, :4] == amp[:, 0:-1:2, :4]).mean() > (inten[:, 1::2, :4] == inten[:, 0:-1:2, :4]).mean() + 0.1
+    pa, pi = O.ks_test(amp, 3, 3), O.ks_test(inten, 3, 3)
+    # ranks agree except at the ties |z| makes
+    same = (pa == pi) | (np.isnan(pa) & np.isnan(pi))
+    assert 0 < (~same).sum() < same.size // 50
