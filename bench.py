@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=160, help="side of the crop timed on the host")
+    ap.add_argument("--stream-chunk", type=int, default=500,
+                    help="lines per chunk of the scene streamed from host memory (0: no streaming run)")
     ap.add_argument("--serve-requests", type=int, default=16, help="tiles in the serving episode (0: none)")
     ap.add_argument("--serve-rate", type=float, default=8.0, help="Poisson arrival rate of tiles per second")
     ap.add_argument("--serve-slots", type=int, default=4, help="tiles in flight at once")
@@ -254,6 +256,32 @@ def precision_variants(cfg, rslc, ref, dev) -> dict:
             "nan_points": int((~fin).sum())}
         del ch, r
     return out
+
+
+# ----------------------------------------------------------------------------- streaming
+def scene_stream(cfg, rslc, ref, chain, args) -> dict:
+    """The scene streamed from a host array through SceneRunner in chunks of full lines with
+    az_half_win halo lines: wall-clock DS px/s with the host reads, copies and results included,
+    and whether the results equal the whole-scene chain's bit for bit."""
+    from moraine_b200.scene import ArraySource, SceneRunner
+    host = rslc.cpu().numpy()
+    runner = SceneRunner(host.shape, cfg.az_half_win, cfg.r_half_win, chunks=(args.stream_chunk, -1),
+                         p_max=cfg.p_max, min_shp=cfg.min_shp, precision=args.precision,
+                         emi_precision=chain.emi_precision, device=rslc.device)
+    src = ArraySource(host)
+    runner.run(src, return_shp_num=False)  # warm-up
+    out = runner.run(src, return_shp_num=False)
+    same = (out.n_ds == ref.n_ds and np.array_equal(out.idx, ref.idx.cpu().numpy())
+            and np.array_equal(out.t_coh.view(np.uint32), ref.t_coh.cpu().numpy().view(np.uint32)))
+    st = out.stats
+    log(f"scene stream: {len(runner.tiles)} tiles of {runner.tile_shape}, {st['wall_s'] * 1e3:.0f} ms, "
+        f"same as whole scene: {same}")
+    del runner
+    torch.cuda.empty_cache()
+    return {"value": out.n_ds / st["wall_s"], "unit": UNIT, "wall_ms": st["wall_s"] * 1e3,
+            "chunks": [args.stream_chunk, -1], "tiles": st["tiles"], "tile_shape": list(st["tile_shape"]),
+            "read_bytes": st["read_bytes"], "n_ds": out.n_ds, "same_as_whole_scene": bool(same),
+            "path": "moraine_b200.scene.SceneRunner over a host numpy stack (wall clock, results on the host)"}
 
 
 # ----------------------------------------------------------------------------- serving
@@ -517,6 +545,11 @@ def main():
                "h2d_bytes_per_step": int(rslc.numel() * 8), "d2h_bytes_per_step": int(d2h + 8),
                "path": "moraine_b200.chain.DsChain.run on a pinned host stack, results copied back"}
 
+    # the scene streamed from host memory in halo tiles (reads, copies and compute overlapped)
+    stream = None
+    if not args.no_variants and world == 1 and args.stream_chunk > 0:
+        stream = scene_stream(cfg, rslc, res, chain, args)
+
     # precision variants on the same stack, against the headline's FP64 chain
     variants = None
     # single-GPU reports (precision variants, serving): only at N = 1, so that ranks stay in step
@@ -560,7 +593,7 @@ def main():
             "vs_baseline": None, "dtype": DTYPE[args.precision], "data": "synthetic",
             "config": workload, "n_ds_per_gpu": n_ds, "stage_ms": stage, "roofline": roofline,
             "stage_roofline": stage_roof, "precision_variants": variants,
-            "cpu_baseline": cpu, "e2e": e2e, "latency": latency, "clocks": clk, "gpu_launches": launches,
+            "cpu_baseline": cpu, "e2e": e2e, "scene_stream": stream, "latency": latency, "clocks": clk, "gpu_launches": launches,
         }))
     if world > 1:
         dist.destroy_process_group()

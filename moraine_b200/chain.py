@@ -120,8 +120,8 @@ class DsChain:
         nlines, width, n = self.shape
         _lib.call("mr_ds_chain_async", self.x.data_ptr(), nlines, width, n, self.azh, self.rh,
                   _lib.KS_INPUT[self.ks_input], self.p_max, self.min_shp, self.prec, self.emi_prec,
-                  self.idx.data_ptr(), self.ph.data_ptr(), self.quality.data_ptr(), self.t_coh.data_ptr(), nlines * width, self.n_ds_g.data_ptr(), self.batch, self.g_base,
-                  self.g_bytes, _dev.stream())
+                  self.idx.data_ptr(), self.ph.data_ptr(), self.quality.data_ptr(), self.t_coh.data_ptr(),
+                  nlines * width, self.n_ds_g.data_ptr(), self.batch, self.g_base, self.g_bytes, _dev.stream())
 
     def _run_graph(self, rslc: torch.Tensor) -> ChainResult:
         self.x.copy_(rslc)
@@ -136,12 +136,21 @@ class DsChain:
         n_ds = int(self.n_ds_g.item())
         return ChainResult(n_ds, self.idx[:n_ds], self.ph[:n_ds], self.quality[:n_ds], self.t_coh[:n_ds], None, None)
 
-    def run(self, rslc: torch.Tensor) -> ChainResult:
+    def run(self, rslc: torch.Tensor, own: tuple[int, int, int, int] | None = None) -> ChainResult:
+        """The chain on one stack. ``own = (line0, line1, pixel0, pixel1)`` limits the DS points to
+        that part of the stack (a tile's region without its halo); the masks and counts are
+        still computed for every pixel, the counts outside ``own`` are then set to 0."""
         nlines, width, n = self.shape
         if tuple(rslc.shape) != self.shape or rslc.dtype != torch.complex64 or not rslc.is_cuda:
             raise ValueError(f"DsChain.run: expected a CUDA complex64 stack of shape {self.shape}, got "
                              f"{rslc.dtype} {tuple(rslc.shape)} on {rslc.device}")
         rslc = rslc.contiguous()
+        if own is not None:
+            l0, l1, p0, p1 = (int(v) for v in own)
+            if not (0 <= l0 <= l1 <= nlines and 0 <= p0 <= p1 <= width):
+                raise ValueError(f"DsChain.run: own {own} is not inside the {nlines} x {width} stack")
+            if self.graph:
+                raise ValueError("DsChain.run: own is not available in graph mode")
         if self.graph:
             return self._run_graph(rslc)
         s = _dev.stream()
@@ -159,6 +168,11 @@ class DsChain:
         mark("intensity")
         _lib.call("mr_ks_test", self.rmli.data_ptr(), nlines, width, n, self.azh, self.rh, None, None, self.p_max,
                   self.is_shp.data_ptr(), self.shp_num.data_ptr(), self.ks_ws.data_ptr(), self.ks_ws.numel(), s)
+        if own is not None and (l0, l1, p0, p1) != (0, nlines, 0, width):
+            self.shp_num[:l0].zero_()
+            self.shp_num[l1:].zero_()
+            self.shp_num[l0:l1, :p0].zero_()
+            self.shp_num[l0:l1, p1:].zero_()
         mark("ks_select")
         npix = nlines * width
         _lib.call("mr_ds_extract", self.shp_num.data_ptr(), None, nlines, width, self.win, self.min_shp,

@@ -220,6 +220,34 @@ def ps_small(src: str, rng):
                         calamp=cal.calamp(amp0))
 
 
+CHUNK_CASES = [((10, 7), (4, -1), (2, 1)), ((2000, 2000), (500, 512), (5, 10)), ((97, 53), (16, 16), (7, 15)),
+               ((5, 5), (8, 8), (2, 2)), ((33, 40), (1, 40), (0, 0)), ((20, 18, 5), (8, 6, -1), (2, 3, 0)),
+               ((64, 64), (13, 9), (20, 20))]
+
+
+def chunk_small(src: str):
+    """moraine/chunk_.py:62-118: all_chunk_slices_with_overlap and chunkwise_slicing_mapping, the
+    halo tiling of dask_from_zarr_overlap (moraine/cli/dask_.py:116) and trim_overlap."""
+    sys.modules.setdefault("moraine", types.ModuleType("moraine")).__path__ = [str(Path(src) / "moraine")]
+    rt = types.ModuleType("moraine.rtree")  # chunk_ imports HilbertRtree for its point-cloud helpers only
+    rt.HilbertRtree = None
+    sys.modules["moraine.rtree"] = rt
+    spec = importlib.util.spec_from_file_location("moraine.chunk_", str(Path(src) / "moraine" / "chunk_.py"))
+    ch = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(ch)
+
+    def arr(slices):
+        return np.array([[[sl.start, sl.stop] for sl in t] for t in slices], dtype=np.int64)
+
+    out = {}
+    for k, (shape, chunks, depths) in enumerate(CHUNK_CASES):
+        out[f"case{k}"] = np.array([shape, chunks, depths], dtype=np.int64)
+        out[f"overlap{k}"] = arr(ch.all_chunk_slices_with_overlap(shape, chunks, depths))
+        i, o, m = ch.chunkwise_slicing_mapping(shape, chunks, depths)
+        out[f"in{k}"], out[f"out{k}"], out[f"map{k}"] = arr(i), arr(o), arr(m)
+    np.savez_compressed(HERE / "chunk_small.npz", **out)
+
+
 def main():
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     src = args[0] if args else "/root/reference"
@@ -229,6 +257,9 @@ def main():
     if "--ps-only" in sys.argv:
         ps_small(src, np.random.default_rng(20240603))
         return
+    if "--chunk-only" in sys.argv:
+        chunk_small(src)
+        return
     mr = load_reference(src)
     rng = np.random.default_rng(20240601)
     ks_tables(mr)
@@ -237,6 +268,7 @@ def main():
     chain_small(mr)
     gamma_small(src, np.random.default_rng(20240602))
     ps_small(src, np.random.default_rng(20240603))
+    chunk_small(src)
     import numba  # noqa: PLC0415
 
     (HERE / "MANIFEST.txt").write_text(
