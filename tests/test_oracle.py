@@ -166,3 +166,37 @@ def test_ks_input_choice_changes_ties():
     # ranks agree except at the ties |z| makes
     same = (pa == pi) | (np.isnan(pa) & np.isnan(pi))
     assert 0 < (~same).sum() < same.size // 50
+
+
+def _ks_p_float32_path(n: int) -> np.ndarray:
+    """The p table of the reference's CUDA kernel (moraine/shp.py:166-197, T = float32):
+    dmax = k / N in float32, x = (en + 0.12 + 0.11 / en) * dmax in double rounded to float32,
+    x2 = -2 x^2, terms summed in float32. numpy's float32 exp stands in for CUDA's expf
+    (both within a few ulp of exp), so this is the path's value up to that rounding."""
+    en = np.sqrt(np.float32(n) / np.float32(2))
+    out = np.empty(n + 1, np.float32)
+    for k in range(n + 1):
+        dmax = np.abs(np.float32(k) / np.float32(n))
+        x = np.float32((float(en) + 0.12 + 0.11 / float(en)) * float(dmax))
+        x2 = np.float32(-2.0 * float(x) * float(x))
+        p = p2 = np.float32(0)
+        sign = 1
+        for i in range(1, 101):
+            p = np.float32(p + np.float32(sign * 2) * np.exp(np.float32(np.float32(x2 * np.float32(i)) * np.float32(i))))
+            if p == p2:
+                break
+            sign = -sign
+            p2 = p
+        out[k] = p
+    return out
+
+
+def test_ks_p_meets_the_gpu_path_tolerance():
+    """The reference checks its CUDA kernel against its Numba path with dist equal and p
+    almost equal to 6 decimals (nbs/API/shp.ipynb, the cupy comparison cells). The p table here
+    follows the Numba path bit for bit, so it must sit within that tolerance of the CUDA
+    kernel's float32 formula for every N and k, with the same SHP decisions at p_max = 0.05."""
+    for n in list(range(2, 81)) + [96, 100, 128, 150, 200, 256, 300, 400, 512]:
+        f64, f32 = O.ks_p_table(n), _ks_p_float32_path(n)
+        assert np.abs(f64.astype(np.float64) - f32).max() < 1.5e-6, n
+        np.testing.assert_array_equal(f64.astype(np.float64) < 0.05, f32.astype(np.float64) < 0.05, err_msg=str(n))
