@@ -245,6 +245,22 @@ int mr_emi_routed(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, d
                   mr_complex64* ph, float* emi_quality, float* t_coh, uint8_t* route,
                   void* workspace, size_t workspace_bytes, mr_stream_t stream);
 
+/* ---------------------------------------------------------------- raster <-> point cloud
+ * Replace moraine.pc.ras2pc (moraine/pc.py:239-241: pc = ras[gix[:, 0], gix[:, 1]]) and
+ * moraine.pc.pc2ras with a grid index (moraine/pc.py:223-236: a raster filled with NaN, then
+ * ras[gix[:, 0], gix[:, 1]] = pc). A record is one pixel's trailing dimensions, elem_bytes
+ * long (the raster is (nlines, width, record), the point cloud (n, record)); gix is (n, 2)
+ * int32 (line, pixel) with numpy's index rules (-nlines <= line < nlines, negative from the
+ * end; the same for pixels). An index outside that range sets *err (device int) to 1 and its
+ * point is skipped; the caller clears *err first and reads it afterwards. pc2ras first sets
+ * every record to the fill pattern (fill: fill_bytes = 4, 8 or 16 host bytes, repeated; 0 =
+ * no fill), then scatters; with repeated indices one of the records lands, unspecified which. */
+int mr_ras2pc(const void* ras, int64_t nlines, int64_t width, int64_t elem_bytes,
+              const int32_t* gix, int64_t n, void* pc, int* err, mr_stream_t stream);
+int mr_pc2ras(const void* pc, const int32_t* gix, int64_t n, int64_t nlines, int64_t width,
+              int64_t elem_bytes, const void* fill, int fill_bytes, void* ras, int* err,
+              mr_stream_t stream);
+
 /* ---------------------------------------------------------------- the whole chain
  * Replaces the stage drivers moraine/cli/shp.py:33 (ks_test, select_shp), the DS selection
  * of nbs/API/pl.ipynb#cell15, moraine/cli/co.py:33 (emperical_co_pc) and

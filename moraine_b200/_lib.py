@@ -37,6 +37,8 @@ _SIGNATURES = {
     "mr_ds_chain_async": (c_int, [P, c_int, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_int, c_int, P, P, P,
                                   P, c_int64, P, c_int64, P, c_size_t, P]),
     "mr_rslc2amp": (c_int, [P, c_int64, P, P]),
+    "mr_ras2pc": (c_int, [P, c_int64, c_int64, c_int64, P, c_int64, P, P, P]),
+    "mr_pc2ras": (c_int, [P, P, c_int64, c_int64, c_int64, c_int64, P, c_int, P, P, P]),
     "mr_amp_disp": (c_int, [P, c_int64, c_int, P, P]),
     "mr_calamp_workspace_bytes": (c_size_t, []),
     "mr_calamp": (c_int, [P, c_int64, P, P, c_size_t, P]),
