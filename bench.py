@@ -263,6 +263,8 @@ def scene_stream(cfg, rslc, ref, chain, args) -> dict:
     """The scene streamed from a host array through SceneRunner in chunks of full lines with
     az_half_win halo lines: wall-clock DS px/s with the host reads, copies and results included,
     and whether the results equal the whole-scene chain's bit for bit."""
+    import torch  # noqa: PLC0415
+
     from moraine_b200.scene import ArraySource, SceneRunner
     host = rslc.cpu().numpy()
     runner = SceneRunner(host.shape, cfg.az_half_win, cfg.r_half_win, chunks=(args.stream_chunk, -1),
