@@ -100,6 +100,54 @@ def test_stream_equals_whole_scene(chunks, azh, rh):
     assert res.stats["tiles"] == len(runner.tiles)
 
 
+def _band_rank(rank, world, port, out_path):
+    """One rank of a two-rank gloo run: its azimuth band (moraine_b200.shard) streamed in halo
+    tiles, the DS points of the lines it owns gathered to rank 0 and compared with the whole
+    scene."""
+    import os
+
+    import torch.distributed as dist
+
+    from moraine_b200.shard import band_partition, owned, to_scene
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        z = _scene()
+        azh, rh, ms = 2, 3, 11
+        band = band_partition(z.shape[0], world, azh)[rank]
+        zb = np.ascontiguousarray(z[band.read0:band.read1])
+        runner = SceneRunner(zb.shape, azh, rh, chunks=(6, 10), device="cpu",
+                             chain_factory=lambda ty, tx, n: FakeChain(ty, tx, n, azh, rh, ms))
+        res = runner.run(ArraySource(zb))
+        keep = owned(torch.from_numpy(res.idx), band).numpy()
+        part = (to_scene(torch.from_numpy(res.idx[keep]), band).numpy(), res.ph[keep], res.quality[keep])
+        parts = [None] * world
+        dist.all_gather_object(parts, part)  # result collection only: no exchange on the data path
+        if rank == 0:
+            whole = FakeChain(*z.shape, azh, rh, ms).run(torch.from_numpy(z))
+            np.testing.assert_array_equal(np.concatenate([q[0] for q in parts]), whole.idx.numpy())
+            np.testing.assert_array_equal(np.concatenate([q[1] for q in parts]).view(np.uint32),
+                                          whole.ph.numpy().view(np.uint32))
+            np.testing.assert_array_equal(np.concatenate([q[2] for q in parts]), whole.quality.numpy())
+            with open(out_path, "w") as f:
+                f.write(f"ok {whole.n_ds}")
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_stream_their_bands(tmp_path):
+    import socket
+
+    import torch.multiprocessing as mp
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    out = tmp_path / "ok.txt"
+    mp.start_processes(_band_rank, args=(2, port, str(out)), nprocs=2, join=True, start_method="spawn")
+    assert out.read_text().startswith("ok ")
+
+
 def test_sources_check_shapes(tmp_path):
     z = _scene()
     with pytest.raises(ValueError):
