@@ -42,6 +42,7 @@ class TileRequest:
     min_shp: int = 50
     precision: str = "fp64"             # coherence Gram arithmetic
     emi_precision: str | None = None    # EMI arithmetic (default: follows the Gram)
+    ks_input: str = "intensity"         # what the KS test ranks: "intensity" |z|^2 or "amplitude" |z|
     request_id: int = 0
     arrival: float | None = None   # time.perf_counter() of arrival; set by submit() if None
 
@@ -200,12 +201,14 @@ class DsServer:
 
     def _run_chain(self, req: TileRequest, plan: dict, stream) -> dict:
         nl, w, n = req.rslc.shape
-        key = (nl, w, n, req.az_half_win, req.r_half_win, req.p_max, req.min_shp, req.precision, req.emi_precision)
+        key = (nl, w, n, req.az_half_win, req.r_half_win, req.p_max, req.min_shp, req.precision, req.emi_precision,
+               req.ks_input)
         chain = plan.get(key)
         if chain is None:
             plan.clear()  # one plan per slot: a new shape frees the previous buffers
             chain = DsChain(nl, w, n, req.az_half_win, req.r_half_win, req.p_max, req.min_shp,
-                            precision=req.precision, emi_precision=req.emi_precision, device=self.device)
+                            precision=req.precision, emi_precision=req.emi_precision, ks_input=req.ks_input,
+                            device=self.device)
             plan[key] = chain
         x = req.rslc
         if not x.is_cuda:
