@@ -51,3 +51,41 @@ def test_host_validation_without_gpu(call, code):
     lib = _lib.load()
     assert call(lib) == code
     assert _lib.last_error()
+
+
+C_HOST = r"""
+#include <stdio.h>
+#include <string.h>
+#include "moraine_b200.h"
+
+int main(void) {
+  /* host-side paths only: no device memory, no kernel */
+  if (mr_abi_version() != 2) return 1;
+  if (mr_gamma_sample_bytes(MR_GAMMA_FCOMPLEX) != 8) return 2;
+  if (mr_ks_workspace_bytes(100, 100, 17) == 0) return 3;
+  if (mr_ds_chain_workspace_bytes(64, 64, 20, 2, 3, 1000) == 0) return 4;
+  int rc = mr_ks_test(NULL, 10, 10, 17, 1, 1, NULL, NULL, 0.05, NULL, NULL, NULL, 0, NULL);
+  if (rc != MR_ERR_INVALID || strlen(mr_last_error()) == 0) return 5;
+  printf("ok %s\n", mr_last_error());
+  return 0;
+}
+"""
+
+
+def test_header_binds_from_plain_c(tmp_path):
+    """A C99 host (no Python, no C++) compiles against the header with -pedantic -Werror,
+    links the library and gets its status codes and messages."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "host.c"
+    src.write_text(C_HOST)
+    exe = tmp_path / "host"
+    libdir = Path(_lib.load()._name).parent
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", f"-I{HEADER.parent}", str(src),
+                    f"-L{libdir}", "-lmoraine_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, (out.returncode, out.stdout, out.stderr)
+    assert out.stdout.startswith("ok ") and "ks_test" in out.stdout
