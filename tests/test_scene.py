@@ -235,3 +235,32 @@ def test_device_stream_from_memmap_and_gamma(cuda, tmp_path):
         z[:, :, d].astype(">c8").tofile(p)
         paths.append(str(p))
     _assert_same(runner.run(GammaSource(paths, z.shape[1])), whole)
+
+
+def test_chunk_slices_properties():
+    """For any scene, chunk size and depth: the chunks tile the scene exactly, each tile reads
+    its chunk plus the depth on both sides clipped to the scene, and ``inner`` locates the
+    chunk inside what is read."""
+    from hypothesis import given, settings
+    from hypothesis import strategies as st
+
+    @settings(max_examples=200, deadline=None)
+    @given(st.integers(1, 60), st.integers(1, 60), st.integers(-1, 70), st.integers(-1, 70), st.integers(0, 12),
+           st.integers(0, 12))
+    def check(nl, w, cl, cw, dl, dw):
+        if cl == 0 or cw == 0:
+            return
+        tiles = chunk_slices((nl, w), (cl, cw), (dl, dw))
+        cover = np.zeros((nl, w), np.int32)
+        for t in tiles:
+            (o0, o1), (p0, p1) = t.own
+            cover[o0:o1, p0:p1] += 1
+            for (r0, r1), (a0, a1), (i0, i1), n, d in zip(t.read, t.own, t.inner, (nl, w), (dl, dw)):
+                assert (r0, r1) == (max(a0 - d, 0), min(a1 + d, n))
+                assert (i0, i1) == (a0 - r0, a1 - r0)
+        assert (cover == 1).all()
+        # row-major over the chunk grid: chunk rows in order, chunks left to right within a row
+        keys = [(t.own[0][0], t.own[1][0]) for t in tiles]
+        assert keys == sorted(keys)
+
+    check()
