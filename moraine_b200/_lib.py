@@ -6,6 +6,7 @@ no CPU fallback: if the library or a CUDA device is missing, every call raises.
 from __future__ import annotations
 
 import ctypes
+import threading
 from ctypes import c_double, c_int, c_int64, c_size_t, c_void_p
 from pathlib import Path
 
@@ -64,6 +65,7 @@ _SIGNATURES = {
 }
 
 _lib = None
+_load_lock = threading.Lock()  # serving slots may load the library from several threads
 
 
 class MoraineError(RuntimeError):
@@ -77,7 +79,11 @@ def exported_symbols() -> list[str]:
 def load() -> ctypes.CDLL:
     """Load the library (no CUDA context is created by loading)."""
     global _lib
-    if _lib is None:
+    if _lib is not None:
+        return _lib
+    with _load_lock:
+        if _lib is not None:
+            return _lib
         if not LIB_PATH.exists():
             raise RuntimeError(
                 f"moraine_b200 CUDA library not built ({LIB_PATH}); run `python -m moraine_b200.build`")
@@ -90,7 +96,7 @@ def load() -> ctypes.CDLL:
         # synchronisation, then the fastest plan; results do not depend on it
         lib.mr_set_autotune(1)
         _lib = lib
-    return _lib
+        return _lib
 
 
 def last_error() -> str:
