@@ -24,28 +24,30 @@ int fail(int code, const char* fmt, ...) {
   return code;
 }
 
+// Per-device attribute caches; several host threads may fill an entry at once, all with
+// the same value, so the entries are atomics.
 int sm_count() {
-  static int cached[64] = {0};
+  static std::atomic<int> cached[64];
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-  if (cached[dev] == 0) {
-    int n = 0;
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
-    cached[dev] = n;
+  int c = cached[dev].load(std::memory_order_relaxed);
+  if (c == 0) {
+    if (cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || c <= 0) c = 148;
+    cached[dev].store(c, std::memory_order_relaxed);
   }
-  return cached[dev];
+  return c;
 }
 
 int smem_optin() {
-  static int cached[64] = {0};
+  static std::atomic<int> cached[64];
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
-  if (cached[dev] == 0) {
-    int n = 0;
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) n = 0;
-    cached[dev] = n;
+  int c = cached[dev].load(std::memory_order_relaxed);
+  if (c == 0) {
+    if (cudaDeviceGetAttribute(&c, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) c = 0;
+    cached[dev].store(c, std::memory_order_relaxed);
   }
-  return cached[dev];
+  return c;
 }
 
 int allow_smem(const void* kernel, size_t bytes) {
