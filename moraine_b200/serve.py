@@ -85,6 +85,9 @@ def latency_summary(results: list[TileResult]) -> dict:
             "n_ds": n_ds, "span_s": last - first, "ds_pixels_per_s": n_ds / max(last - first, 1e-9)}
 
 
+_DROP = "drop"  # _take's answer to a slot whose kept memory blocks the head request
+
+
 class _Item:
     __slots__ = ("req", "fut", "fp")
 
@@ -97,10 +100,17 @@ class DsServer:
 
     ``runner`` replaces the device chain (``runner(request, stream) -> TileResult fields``);
     it exists for tests of the admission logic without a GPU.
+
+    Accounting: a slot keeps its plan (the chain's buffers) for the next tile of the same
+    shape, and the memory it freed stays in its stream's pool of the caching allocator, so
+    an idle slot still holds device memory. Each slot is therefore charged the larger of
+    what it held before and its running tile's footprint, and keeps that charge when the
+    tile ends (``keep_slot_memory``, on for the device chain, off for ``runner``).
     """
 
     def __init__(self, hbm_budget: float = 150e9, slots: int = 4, device=None,
-                 runner: Callable | None = None, footprint_fn: Callable = footprint):
+                 runner: Callable | None = None, footprint_fn: Callable = footprint,
+                 keep_slot_memory: bool | None = None):
         self.budget = int(hbm_budget)
         self.slots = int(slots)
         self.used = 0
@@ -113,6 +123,9 @@ class DsServer:
         self._closed = False
         self._footprint = footprint_fn
         self._runner = runner
+        self._keep = (runner is None) if keep_slot_memory is None else bool(keep_slot_memory)
+        self._charge = [0] * self.slots  # what each slot counts in self.used
+        self._idle: set[int] = set()     # slots waiting for a request
         if runner is None:
             self.device = torch.device(device) if device is not None else torch.device("cuda",
                                                                                        torch.cuda.current_device())
@@ -153,24 +166,51 @@ class DsServer:
         self.close()
 
     # -------------------------------------------------------------- slots
-    def _take(self) -> _Item | None:
-        with self._cv:
-            while True:
-                if self._queue and self.used + self._queue[0].fp <= self.budget:
-                    item = self._queue.popleft()  # arrival order: the head is admitted first
-                    self.used += item.fp
-                    self.active += 1
-                    self.peak_used = max(self.peak_used, self.used)
-                    self.peak_active = max(self.peak_active, self.active)
-                    self.admitted_order.append(item.req.request_id)
-                    return item
-                if self._closed and not self._queue:
-                    return None
-                self._cv.wait()
+    def _fits(self, slot: int) -> bool:
+        held = self._charge[slot]
+        return self.used - held + max(held, self._queue[0].fp) <= self.budget
 
-    def _release(self, item: _Item) -> None:
+    def _take(self, slot: int):
+        """The next request for this slot; None when the server closes; _DROP when the head
+        request is blocked by memory that idle slots keep, this one's included: the slot then
+        gives its memory back (``_drop``) and asks again."""
         with self._cv:
-            self.used -= item.fp
+            self._idle.add(slot)
+            try:
+                while True:
+                    held = self._charge[slot]
+                    if self._queue and self._fits(slot):
+                        item = self._queue.popleft()  # arrival order: the head is admitted first
+                        self._charge[slot] = max(held, item.fp)
+                        self.used += self._charge[slot] - held
+                        self.active += 1
+                        self.peak_used = max(self.peak_used, self.used)
+                        self.peak_active = max(self.peak_active, self.active)
+                        self.admitted_order.append(item.req.request_id)
+                        return item
+                    if self._closed and not self._queue:
+                        return None
+                    if self._queue and held > 0 and not any(self._fits(o) for o in self._idle):
+                        return _DROP
+                    self._cv.wait()
+            finally:
+                self._idle.discard(slot)
+
+    def _drop(self, slot: int, plan: dict) -> None:
+        """Free this slot's kept memory (its plan and its stream's cached blocks) and its charge."""
+        plan.clear()
+        if self._runner is None:
+            torch.cuda.empty_cache()
+        with self._cv:
+            self.used -= self._charge[slot]
+            self._charge[slot] = 0
+            self._cv.notify_all()
+
+    def _release(self, item: _Item, slot: int) -> None:
+        with self._cv:
+            if not self._keep:
+                self.used -= self._charge[slot]
+                self._charge[slot] = 0
             self.active -= 1
             self._cv.notify_all()
 
@@ -181,9 +221,12 @@ class DsServer:
             stream = torch.cuda.Stream(self.device)
         plan: dict = {}
         while True:
-            item = self._take()
+            item = self._take(slot)
             if item is None:
                 return
+            if item is _DROP:
+                self._drop(slot, plan)
+                continue
             admitted = time.perf_counter()
             try:
                 if self._runner is not None:
@@ -197,7 +240,7 @@ class DsServer:
             except BaseException as e:  # noqa: BLE001 - handed to the caller's future
                 item.fut.set_exception(e)
             finally:
-                self._release(item)
+                self._release(item, slot)
 
     def _run_chain(self, req: TileRequest, plan: dict, stream) -> dict:
         nl, w, n = req.rslc.shape

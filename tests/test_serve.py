@@ -151,3 +151,20 @@ def test_results_same_alone_and_in_mix(cuda):
         assert torch.equal(a.t_coh.view(torch.int32), m.t_coh.view(torch.int32))
     s = latency_summary(list(mixed.values()))
     assert s["requests"] == len(reqs) and s["p99_ms"] >= s["p50_ms"] > 0
+
+
+def test_kept_slot_memory_is_charged_and_given_back():
+    """With slots keeping their memory between tiles (the device chain's plans and cached
+    blocks), each slot is charged what it keeps; a request that the kept memory blocks makes
+    the idle slots give theirs back instead of waiting for ever."""
+    log, lock = [], threading.Lock()
+    sizes = {0: 60, 1: 40, 2: 70, 3: 30, 4: 90, 5: 10}
+    srv = DsServer(hbm_budget=100, slots=2, runner=_fake_runner(log, lock, hold=0.05),
+                   footprint_fn=lambda r: sizes[r.request_id], keep_slot_memory=True)
+    futs = [srv.submit(_req(i)) for i in sizes]
+    res = [f.result(timeout=30) for f in futs]
+    srv.close()
+    assert [r.request_id for r in res] == list(sizes)
+    assert srv.peak_used <= 100
+    assert 0 < srv.used <= 100 and srv.used == sum(srv._charge)  # kept after the last tiles
+    assert srv.admitted_order == list(sizes)
