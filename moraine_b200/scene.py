@@ -153,6 +153,7 @@ class GammaSource:
 # ----------------------------------------------------------------------------- runner
 @dataclass
 class SceneResult:
+    """Whole-scene results (None when ``run`` was given a sink)."""
     n_ds: int
     idx: np.ndarray             # (n_ds, 2) int32 scene (line, pixel), row-major order
     ph: np.ndarray              # (n_ds, nimages) complex64
@@ -160,6 +161,18 @@ class SceneResult:
     t_coh: np.ndarray           # (n_ds,) float32
     shp_num: np.ndarray | None  # (nlines, width) int32
     stats: dict = field(default_factory=dict)
+
+
+@dataclass
+class SceneRows:
+    """The results of one chunk row (``lines`` = (first, stop) scene lines it owns), handed to
+    ``SceneRunner.run``'s ``sink`` in scene order."""
+    lines: tuple
+    idx: np.ndarray             # (n, 2) int32 scene (line, pixel), row-major order
+    ph: np.ndarray              # (n, nimages) complex64
+    quality: np.ndarray         # (n,) float32
+    t_coh: np.ndarray           # (n,) float32
+    shp_num: np.ndarray | None  # (lines[1] - lines[0], width) int32
 
 
 class SceneRunner:
@@ -187,8 +200,13 @@ class SceneRunner:
         self.chain = chain_factory(ty, tx, nimages)
         self.device = torch.device(getattr(self.chain, "device", device or "cpu"))
 
-    def run(self, source, return_shp_num: bool = True) -> SceneResult:
-        """All tiles of ``source`` through the chain; results on the host in scene row-major order."""
+    def run(self, source, return_shp_num: bool = True, sink=None) -> SceneResult:
+        """All tiles of ``source`` through the chain; results on the host in scene row-major order.
+
+        With ``sink`` (a callable), the results are not gathered: each chunk row's are handed
+        to ``sink(SceneRows)`` in scene order, one row behind the device so that its copies
+        are done without stalling the stream (the reference writes each chunk to its zarr
+        store the same way), and the returned ``SceneResult`` holds only counts and stats."""
         if tuple(source.shape) != self.shape:
             raise ValueError(f"SceneRunner.run: source has shape {tuple(source.shape)}, the plan {self.shape}")
         nlines, width, n = self.shape
@@ -210,7 +228,25 @@ class SceneRunner:
             source.stage(t.read[0], t.read[1], hosts[slot])
 
         pending, shp_parts, row = [], [], []
+        waiting = []  # chunk rows copied to the host, not yet handed to the sink
+        delivered = 0
         read_bytes = 0
+        empty = (np.empty((0, 2), np.int32), np.empty((0, n), np.complex64), np.empty((0,), np.float32),
+                 np.empty((0,), np.float32))
+
+        def deliver(entry) -> int:
+            lines, parts, shp_row, ev = entry
+            if ev is not None:
+                ev.synchronize()
+            arrays = tuple(x.numpy() for x in parts) if parts is not None else empty
+            shp = None
+            if shp_row is not None:
+                shp = np.empty((lines[1] - lines[0], width), np.int32)
+                for (rows, cols), part in shp_row:
+                    shp[rows[0] - lines[0]:rows[1] - lines[0], cols[0]:cols[1]] = part.numpy()
+            sink(SceneRows(lines, *arrays, shp))
+            return len(arrays[0])
+
         pool = ThreadPoolExecutor(max_workers=1)
         try:
             fut = pool.submit(stage, 0)
@@ -247,13 +283,31 @@ class SceneRunner:
                     ev.record()
                     consumed[slot] = ev
                 if k + 1 == len(self.tiles) or self.tiles[k + 1].own[0] != t.own[0]:
-                    if row:
-                        pending.append(self._merge_row(row, width, cuda))
+                    if sink is None:
+                        if row:
+                            pending.append(self._merge_row(row, width, cuda))
+                    else:
+                        parts = self._merge_row(row, width, cuda) if row else None
+                        ev = None
+                        if cuda:
+                            ev = torch.cuda.Event()
+                            ev.record()
+                        waiting.append((t.own[0], parts, shp_parts if return_shp_num else None, ev))
+                        shp_parts = []
+                        while len(waiting) > 1:  # the row before this one: its copies are done
+                            delivered += deliver(waiting.pop(0))
                     row = []
         finally:
             pool.shutdown(wait=True)
+        while waiting:
+            delivered += deliver(waiting.pop(0))
         if cuda:
             torch.cuda.current_stream(dev).synchronize()
+        if sink is not None:
+            wall = time.perf_counter() - t0
+            stats = dict(tiles=len(self.tiles), tile_shape=self.tile_shape, read_bytes=read_bytes, wall_s=wall,
+                         ds_per_s=delivered / wall if wall > 0 else 0.0)
+            return SceneResult(delivered, None, None, None, None, None, stats)
         n_ds = sum(len(p[0]) for p in pending)
         cat = (lambda i, dt, tail: np.concatenate([p[i].numpy() for p in pending]) if pending
                else np.empty((0,) + tail, dt))

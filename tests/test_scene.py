@@ -100,6 +100,29 @@ def test_stream_equals_whole_scene(chunks, azh, rh):
     assert res.stats["tiles"] == len(runner.tiles)
 
 
+@pytest.mark.parametrize("chunks", [(7, 9), (5, -1), (100, 100)])
+def test_sink_gets_chunk_rows_in_scene_order(chunks):
+    """With a sink, each chunk row's results arrive in scene order and together equal the
+    whole-scene run; nothing is gathered."""
+    z = _scene()
+    azh, rh, ms = 2, 3, 11
+    whole = FakeChain(*z.shape, azh, rh, ms).run(torch.from_numpy(z))
+    runner = SceneRunner(z.shape, azh, rh, chunks=chunks, device="cpu",
+                         chain_factory=lambda ty, tx, n: FakeChain(ty, tx, n, azh, rh, ms))
+    rows = []
+    res = runner.run(ArraySource(z), sink=rows.append)
+    assert res.idx is None and res.n_ds == whole.n_ds > 0
+    assert rows[0].lines[0] == 0 and rows[-1].lines[1] == z.shape[0]
+    assert all(a.lines[1] == b.lines[0] for a, b in zip(rows[:-1], rows[1:]))
+    np.testing.assert_array_equal(np.concatenate([r.idx for r in rows]), whole.idx.numpy())
+    np.testing.assert_array_equal(np.concatenate([r.ph for r in rows]).view(np.uint32),
+                                  whole.ph.numpy().view(np.uint32))
+    np.testing.assert_array_equal(np.concatenate([r.quality for r in rows]), whole.quality.numpy())
+    np.testing.assert_array_equal(np.concatenate([r.shp_num for r in rows]), whole.shp_num.numpy())
+    for r in rows:
+        assert ((r.idx[:, 0] >= r.lines[0]) & (r.idx[:, 0] < r.lines[1])).all()
+
+
 def _band_rank(rank, world, port, out_path):
     """One rank of a two-rank gloo run: its azimuth band (moraine_b200.shard) streamed in halo
     tiles, the DS points of the lines it owns gathered to rank 0 and compared with the whole
@@ -218,6 +241,13 @@ def test_device_stream_equals_whole_scene(cuda, chunks, ks_input, emi):
                          min_shp=cfg.min_shp, precision="fp64", emi_precision=emi, ks_input=ks_input, device=cuda)
     assert len(runner.tiles) > 1
     _assert_same(runner.run(ArraySource(z)), whole)
+    rows = []
+    runner.run(ArraySource(z), sink=rows.append)  # chunk rows handed over one by one
+    from types import SimpleNamespace
+    cat = SimpleNamespace(n_ds=sum(len(r.idx) for r in rows), shp_num=np.concatenate([r.shp_num for r in rows]),
+                          **{k: np.concatenate([getattr(r, k) for r in rows]) for k in ("idx", "ph", "quality",
+                                                                                          "t_coh")})
+    _assert_same(cat, whole)
 
 
 @pytest.mark.gpu
