@@ -102,6 +102,57 @@ void oracle_ks_test(const float* rmli, int nlines, int width, int n, int azh, in
   free(sorted);
 }
 
+/* ks_test followed by select_shp (moraine/shp.py:269-323) without the p array: p depends
+ * only on the integer statistic k, so the decision (double)(float)p(k) < p_max is taken
+ * from a table of p over k = 0..n built with the same expression as oracle_ks_test
+ * (moraine/shp.py:74-76, :20-32). is_shp: (nlines, width, az_win, r_win) bytes; shp_num:
+ * (nlines, width) counts. For whole scenes, where the float p array would not fit. */
+void oracle_ks_select(const float* rmli, int nlines, int width, int n, int azh, int rh, double p_max,
+                      uint8_t* is_shp, int32_t* shp_num, int nthreads) {
+  const int64_t npix = (int64_t)nlines * width;
+  const int az_win = 2 * azh + 1, r_win = 2 * rh + 1, win = az_win * r_win;
+  const double en = sqrt((double)n / 2);
+  const double scale = en + 0.12 + 0.11 / en;
+  uint8_t* accept = (uint8_t*)malloc((size_t)n + 1);
+  for (int k = 0; k <= n; ++k) {
+    const double d = fabs((double)k / (double)n);
+    accept[k] = (double)(float)oracle_ks_p(scale * d) < p_max;
+  }
+  float* sorted = (float*)malloc(sizeof(float) * npix * n);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+#endif
+  for (int64_t i = 0; i < npix; ++i) {
+    memcpy(sorted + i * n, rmli + i * n, sizeof(float) * n);
+    qsort(sorted + i * n, n, sizeof(float), cmp_nan_last);
+  }
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+  for (int64_t pix = 0; pix < npix; ++pix) {
+    const int i = (int)(pix / width), j = (int)(pix % width);
+    const float* ref = sorted + pix * n;
+    const int ref_nan = isnan(ref[n - 1]);
+    int32_t count = 0;
+    for (int l = -azh; l <= azh; ++l)
+      for (int m = -rh; m <= rh; ++m) {
+        const int64_t o = pix * win + (l + azh) * r_win + (m + rh);
+        const int si = i + l, sj = j + m;
+        uint8_t a = 0;
+        if (!ref_nan && si >= 0 && si < nlines && sj >= 0 && sj < width) {
+          const float* sec = sorted + ((int64_t)si * width + sj) * n;
+          if (!isnan(sec[n - 1])) a = accept[ks_merge_count(ref, sec, n)];
+        }
+        is_shp[o] = a;
+        count += a;
+      }
+    shp_num[pix] = count;
+  }
+  free(sorted);
+  free(accept);
+}
+
 /* moraine/co.py:209-226 (CPU path, float64 accumulation) and :164-187 (window order).
  * mask: (n_pc, az_win, r_win) bytes; pairs: (npairs, 2) int32; coh: complex128 out. */
 void oracle_co_pc(const float* rslc /* complex64 interleaved */, int nlines, int width, int n,

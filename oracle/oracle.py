@@ -43,6 +43,8 @@ def _load():
         lib.oracle_ks_p.restype = c_double
         lib.oracle_ks_p.argtypes = [c_double]
         lib.oracle_ks_test.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_int]
+        lib.oracle_ks_select.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_int, c_double, c_void_p, c_void_p,
+                                         c_int]
         lib.oracle_co_pc.argtypes = [c_void_p, c_int, c_int, c_int, c_void_p, c_int64, c_void_p, c_int, c_int,
                                      c_void_p, c_int, c_void_p, c_int]
         lib.oracle_co_raster.argtypes = [c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int, c_void_p, c_void_p,
@@ -114,6 +116,18 @@ def select_shp(p: np.ndarray, p_max: float):
     """moraine/shp.py:309-323: is_shp = p < p_max (float32 widened to float64), count per pixel."""
     is_shp = p.astype(np.float64) < float(p_max)
     return is_shp, np.count_nonzero(is_shp, axis=(-2, -1)).astype(np.int32)
+
+
+def ks_select(rmli: np.ndarray, az_half_win: int, r_half_win: int, p_max: float, nthreads: int = 0):
+    """select_shp(ks_test(rmli), p_max) without the float32 p array (whole scenes):
+    is_shp (nlines, width, az_win, r_win) bool and shp_num int32."""
+    rmli = np.ascontiguousarray(rmli, dtype=np.float32)
+    nl, w, n = rmli.shape
+    is_shp = np.empty((nl, w, 2 * az_half_win + 1, 2 * r_half_win + 1), np.uint8)
+    num = np.empty((nl, w), np.int32)
+    _load().oracle_ks_select(_p(rmli), nl, w, n, az_half_win, r_half_win, float(p_max), _p(is_shp), _p(num),
+                             nthreads or nthreads_default())
+    return is_shp.view(bool), num
 
 
 def ds_candidates(is_shp: np.ndarray, shp_num: np.ndarray, min_shp: int):

@@ -1,8 +1,8 @@
 """Generate the golden fixtures of the parity tests from the reference itself.
 
 Runs the reference's own CPU (Numba) functions from a Moraine source checkout — pass its
-path as the first argument (default ``/root/reference``) — on small seeded inputs and
-writes ``tests/golden/*.npz``. Only needed when the fixtures are regenerated; the
+path as the first argument or in the ``MORAINE_REFERENCE`` environment variable — on small
+seeded inputs and writes ``tests/golden/*.npz``. Only needed when the fixtures are regenerated; the
 tests read the committed ``.npz`` files and never import the reference.
 
 Recipe for importing the reference without its optional dependencies: drop
@@ -144,6 +144,33 @@ def chain_small(mr):
                         t_coh_fused=t_f)
 
 
+def chain_images(mr, name: str, side: int, min_shp: int, max_pts: int):
+    """The reference chain on a crop of a benchmark scene model at its own image count
+    (c1: N = 50, 15 x 31 window; c2: N = 100, 11 x 21 window): SHP masks, coherence of the
+    first points, EMI and temporal coherence of at most ``max_pts`` DS points."""
+    sys.path.insert(0, str(REPO))
+    from moraine_b200.synth import CONFIGS, make_stack  # noqa: PLC0415
+
+    base = CONFIGS[name]
+    cfg = base.scaled(nlines=side, width=side, min_shp=min_shp,
+                      n_patches=max(4, round(base.n_patches * side * side / (base.nlines * base.width))))
+    rslc = make_stack(cfg).numpy()
+    re, im = rslc.real.astype(np.float32), rslc.imag.astype(np.float32)
+    rmli = (re * re) + (im * im)
+    p = mr.shp.ks_test(rmli, cfg.az_half_win, cfg.r_half_win)
+    is_shp, shp_num = mr.shp.select_shp(p, cfg.p_max)
+    sel = shp_num >= cfg.min_shp
+    idx = np.stack(np.where(sel), -1)[:max_pts]
+    pc = is_shp[sel][:max_pts]
+    coh = mr.co.emperical_co_pc(rslc, idx, pc)
+    ph, q = mr.pl.emi(coh)
+    t = mr.pl.ds_temp_coh(coh, ph)
+    np.savez_compressed(HERE / f"chain_{name}_n{cfg.nimages}.npz", rslc=rslc,
+                        win=np.array([cfg.az_half_win, cfg.r_half_win]), p_max=np.float64(cfg.p_max),
+                        min_shp=np.int64(cfg.min_shp), is_shp_bits=np.packbits(is_shp.reshape(-1)),
+                        shp_num=shp_num, idx=idx, coh_head=coh[:8], ph=ph, quality=q, t_coh=t)
+
+
 def gamma_samples(rng, dtype: str, count: int) -> np.ndarray:
     """Big-endian samples with the values the no-data rule separates (around 1e-30)."""
     specials = [0.0, -0.0, 1e-31, -1e-31, 9.999999e-31, 1.0000001e-30, 1e-30, -1e-30, 2e-30, 1e-38, 1e-45,
@@ -250,7 +277,15 @@ def chunk_small(src: str):
 
 def main():
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    src = args[0] if args else "/root/reference"
+    src = args[0] if args else os.environ.get("MORAINE_REFERENCE")
+    if not src:
+        sys.exit("usage: make_golden.py <moraine source checkout> [--gamma-only|--ps-only|--chunk-only|--images-only]"
+                 " (or set MORAINE_REFERENCE)")
+    if "--images-only" in sys.argv:
+        mr = load_reference(src)
+        chain_images(mr, "c1", 28, 20, 192)
+        chain_images(mr, "c2", 24, 20, 192)
+        return
     if "--gamma-only" in sys.argv:
         gamma_small(src, np.random.default_rng(20240602))
         return
@@ -266,6 +301,8 @@ def main():
     ks_small(mr, rng)
     co_small(mr, rng)
     chain_small(mr)
+    chain_images(mr, "c1", 28, 20, 192)
+    chain_images(mr, "c2", 24, 20, 192)
     gamma_small(src, np.random.default_rng(20240602))
     ps_small(src, np.random.default_rng(20240603))
     chunk_small(src)

@@ -200,3 +200,47 @@ def test_ks_p_meets_the_gpu_path_tolerance():
         f64, f32 = O.ks_p_table(n), _ks_p_float32_path(n)
         assert np.abs(f64.astype(np.float64) - f32).max() < 1.5e-6, n
         np.testing.assert_array_equal(f64.astype(np.float64) < 0.05, f32.astype(np.float64) < 0.05, err_msg=str(n))
+
+
+@pytest.mark.parametrize("name", ["chain_c1_n50", "chain_c2_n100"])
+def test_oracle_chain_at_benchmark_image_counts(golden, name):
+    """The oracle chain against the reference's own on crops of the benchmark scene models
+    at their image counts (N = 50, 15 x 31 window; N = 100, 11 x 21 window)."""
+    g = golden(f"{name}.npz")
+    rslc = g["rslc"]
+    azh, rh = (int(v) for v in g["win"])
+    p = O.ks_test(O.intensity(rslc), azh, rh)
+    is_shp, num = O.select_shp(p, float(g["p_max"]))
+    np.testing.assert_array_equal(np.packbits(is_shp.reshape(-1)), g["is_shp_bits"])
+    np.testing.assert_array_equal(num, g["shp_num"])
+    idx, pc = O.ds_candidates(is_shp, num, int(g["min_shp"]))
+    k = g["idx"].shape[0]
+    np.testing.assert_array_equal(idx[:k], g["idx"])
+    coh = O.emperical_co_pc(rslc, idx[:k], pc[:k])
+    np.testing.assert_allclose(coh[:8], g["coh_head"], atol=1e-6)
+    c64 = coh.astype(np.complex64)
+    ph, q, gap, cond = O.emi(c64)
+    # the reference's EMI runs complex64 LAPACK: within that arithmetic's bound of FP64
+    tol = O.phase_tolerance(cond, gap, eps=4 * 6e-8)
+    err = np.abs(np.angle(ph * np.conj(g["ph"]))).max(-1)
+    assert np.all(err <= tol), (err / tol).max()
+    assert np.all(np.abs(q - g["quality"]) <= 1e-6 * cond * np.maximum(1, np.abs(q)))
+    # the reference sums the temporal coherence of its own phases in float32
+    np.testing.assert_allclose(O.ds_temp_coh(c64, g["ph"]), g["t_coh"], atol=5e-5)
+
+
+def test_ks_select_equals_ks_test_then_select(golden):
+    """The whole-scene path (table of p over k) decides like ks_test + select_shp."""
+    g = golden("chain_c2_n100.npz")
+    rmli = O.intensity(g["rslc"])
+    azh, rh = (int(v) for v in g["win"])
+    is_shp, num = O.ks_select(rmli, azh, rh, 0.05)
+    ref_m, ref_n = O.select_shp(O.ks_test(rmli, azh, rh), 0.05)
+    np.testing.assert_array_equal(is_shp, ref_m)
+    np.testing.assert_array_equal(num, ref_n)
+    g = golden("ks_small.npz")
+    for tag in ("a", "b", "c"):
+        x, (a, r) = g[f"{tag}_rmli"], g[f"{tag}_win"]
+        m, c = O.ks_select(x, int(a), int(r), 0.05)
+        np.testing.assert_array_equal(m, g[f"{tag}_is_shp"])
+        np.testing.assert_array_equal(c, g[f"{tag}_shp_num"])
