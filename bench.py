@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--emi-precision", default=None, help="EMI arithmetic: fp64, fp32 or mixed (default: fp64 "
                                                           "with an fp64 Gram, else fp32)")
     ap.add_argument("--no-variants", action="store_true", help="skip the precision variants")
+    ap.add_argument("--no-oracle", action="store_true", help="skip the check against the FP64 oracle")
+    ap.add_argument("--oracle-points", type=int, default=10240, help="DS points checked against the oracle")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=160, help="side of the crop timed on the host")
@@ -56,7 +58,12 @@ def parse():
     ap.add_argument("--serve-slots", type=int, default=4, help="tiles in flight at once")
     ap.add_argument("--serve-full", action="store_true",
                     help="full serving workload: tiles up to 2048^2 and nimage up to 150 (default: up to 1024^2, 100)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.steps < 1:
+        ap.error("--steps must be at least 1")
+    if args.impl == "ours" and args.warmup < 1:
+        ap.error("--warmup must be at least 1 (the DS count and the stage split come from a warm-up pass)")
+    return args
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -124,6 +131,14 @@ def measured_peaks() -> dict:
 
 
 DTYPE = {"fp32": "f32", "bf16": "bf16 Gram, f32 EMI", "bf16x3": "bf16x3 Gram, f32 EMI", "fp64": "f64"}
+EMI_DTYPE = {"fp64": "f64", "fp32": "f32", "mixed": "f32 + f64 for cond > 1e4",
+             "refine": "f64 inverse, f32 reduction, f64 refinement and check"}
+
+
+def dtype_of(gram: str, emi: str) -> str:
+    if (gram, emi) in (("fp64", "fp64"), ("fp32", "fp32")):
+        return DTYPE[gram]
+    return f"{DTYPE[gram].split(' Gram')[0]} Gram; EMI {EMI_DTYPE[emi]}"
 
 # DRAM bytes per DS point of one mr_emi call (inverse + reduce + tail kernels), by (N, EMI
 # arithmetic): dram__bytes_read.sum + dram__bytes_write.sum of the three kernels over one
@@ -213,13 +228,15 @@ def stage_rooflines(cfg, stage: dict, n_ds: int, res, peaks: dict, fp32: float, 
 
 # ----------------------------------------------------------------------------- precision
 def precision_variants(cfg, rslc, ref, dev) -> dict:
-    """Time and accuracy of lower-precision chains against the FP64 chain on the same stack.
+    """Time and accuracy of the chain's arithmetic variants against the FP64 chain on the same
+    stack.
 
-    For each variant: DS pixels/s of one pass (after a warm-up pass), the fraction of DS
-    points whose phase history is within 1 mrad of the FP64 chain's, the largest and
-    99th-percentile phase error in rad, the largest temporal-coherence error, the share of
-    points routed to FP64 (mixed EMI), and the largest coherence error over the first
-    20,000 DS points (the Gram alone, against its FP64 accumulation).
+    ``ref`` is the FP64 chain's result. For each variant: DS pixels/s of one pass (after a
+    warm-up pass), the fraction of DS points whose phase history is within 1 mrad of the
+    FP64 chain's, the largest and 99th-percentile phase error in rad, the largest
+    temporal-coherence error, the share of points routed to FP64 (mixed and refined EMI),
+    and the largest coherence error over the first 20,000 DS points (the Gram alone,
+    against its FP64 accumulation).
     """
     import torch  # noqa: PLC0415
 
@@ -231,7 +248,8 @@ def precision_variants(cfg, rslc, ref, dev) -> dict:
     pc = ref.is_shp[idx[:, 0].long(), idx[:, 1].long()].view(torch.bool)
     coh64 = mb.emperical_co_pc(rslc, idx, pc, precision="fp64")
     out = {}
-    for gram, emi in (("fp32", "fp32"), ("fp64", "mixed"), ("fp32", "mixed")):
+    for gram, emi in (("fp32", "fp32"), ("fp64", "fp64"), ("fp64", "fp32"), ("fp64", "refine"),
+                      ("fp64", "mixed")):
         ch = DsChain(cfg.nlines, cfg.width, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp,
                      precision=gram, emi_precision=emi, device=dev)
         ch.run(rslc)
@@ -252,10 +270,65 @@ def precision_variants(cfg, rslc, ref, dev) -> dict:
             "phase_err_p99_rad": float(e[int(0.99 * (e.numel() - 1))]) if e.numel() else None,
             "t_coh_err_max": float((r.t_coh - ref_t).abs()[fin].max()) if e.numel() else None,
             "coh_err_max_abs": float((co - coh64).abs().max()),
-            "routed_to_fp64": float((r.route != 0).float().mean()) if r.route is not None else 0.0,
+            "routed_to_fp64": float((r.route == 1).float().mean()) if r.route is not None else
+            (1.0 if emi == "fp64" else 0.0),
             "nan_points": int((~fin).sum())}
         del ch, r
     return out
+
+
+# ----------------------------------------------------------------------------- oracle check
+def oracle_check(cfg, rslc, res, gram: str, n_points: int = 10240, nthreads: int = 0) -> dict:
+    """The headline chain's results against the FP64 oracle on a seeded sample of DS points.
+
+    For ``n_points`` DS points drawn evenly from the run: the oracle's coherence (C, FP64
+    accumulation) against the device coherence, the oracle's EMI (numpy LAPACK FP64 on that
+    coherence) against the device phases, and the oracle's temporal coherence of the oracle
+    phases against the device value. Reported: the fraction of points within 1 mrad, the
+    median, 99th percentile and largest phase error in rad, the largest coherence and
+    temporal coherence errors.
+    """
+    from concurrent.futures import ThreadPoolExecutor  # noqa: PLC0415
+
+    import torch  # noqa: PLC0415
+    from threadpoolctl import threadpool_limits  # noqa: PLC0415
+
+    import moraine_b200 as mb  # noqa: PLC0415
+    from oracle import oracle as O  # noqa: PLC0415
+
+    nthreads = nthreads or cpu_threads()
+    n = min(n_points, res.n_ds)
+    sel = np.unique(np.linspace(0, res.n_ds - 1, n).round().astype(np.int64))
+    t = torch.from_numpy(sel).to(res.idx.device)
+    idx = res.idx[t]
+    pc = res.is_shp[idx[:, 0].long(), idx[:, 1].long()]
+    coh_dev = mb.emperical_co_pc(rslc, idx, pc.view(torch.bool), precision=gram).cpu().numpy()
+    ph_dev = res.ph[t].cpu().numpy()
+    tc_dev = res.t_coh[t].cpu().numpy()
+    idx_np, pc_np = idx.cpu().numpy(), pc.cpu().numpy().astype(bool)
+    t0 = time.perf_counter()
+    coh = O.emperical_co_pc(rslc.cpu().numpy(), idx_np, pc_np, nthreads=nthreads).astype(np.complex64)
+
+    def emi_part(c):
+        with threadpool_limits(limits=1):
+            return O.emi(c)
+
+    with ThreadPoolExecutor(nthreads) as ex:
+        parts = list(ex.map(emi_part, [coh[i:i + 64] for i in range(0, len(coh), 64)]))
+    ph = np.concatenate([p[0] for p in parts])
+    tc = O.ds_temp_coh(coh, ph.astype(np.complex64), nthreads=nthreads)
+    err = np.abs(np.angle(ph_dev * np.conj(ph))).max(-1)
+    fin = np.isfinite(err)
+    e = np.sort(err[fin])
+    return {"points": int(len(sel)), "frac_within_1mrad": float((err[fin] <= 1e-3).mean()) if fin.any() else None,
+            "phase_err_p99_rad": float(e[int(0.99 * (len(e) - 1))]) if len(e) else None,
+            "phase_err_max_rad": float(e[-1]) if len(e) else None,
+            "phase_err_median_rad": float(np.median(e)) if len(e) else None,
+            "coh_err_max_abs": float(np.abs(coh_dev - coh).max()),
+            "t_coh_err_max": float(np.abs(tc_dev - tc)[fin].max()) if fin.any() else None,
+            "nan_points": int((~fin).sum()), "oracle_s": time.perf_counter() - t0,
+            "oracle": "C FP64 Gram (stored complex64) + numpy LAPACK eigh/inv FP64 + C temporal coherence, "
+                      "DS points drawn evenly over the run"}
 
 
 # ----------------------------------------------------------------------------- streaming
@@ -430,7 +503,8 @@ def main():
             log(f"reference step: {n} DS points in {dt:.1f} s")
         value = float(np.sum(nds) / np.sum(times))
         print(json.dumps({
-            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "note": "one host process (rank 0) on the host cores; the value is not summed over ranks",
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": workload,
@@ -554,9 +628,21 @@ def main():
 
     # precision variants on the same stack, against the headline's FP64 chain
     variants = None
-    # single-GPU reports (precision variants, serving): only at N = 1, so that ranks stay in step
-    if not args.no_variants and world == 1 and args.precision == "fp64" and chain.emi_precision == "fp64":
-        variants = precision_variants(cfg, rslc, res, dev)
+    oracle = None
+    # single-GPU reports (precision variants, oracle check, serving): only at N = 1, so that
+    # ranks stay in step
+    if not args.no_variants and world == 1 and args.precision == "fp64":
+        ref = res
+        if chain.emi_precision != "fp64":
+            ref = DsChain(cfg.nlines, cfg.width, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max,
+                          cfg.min_shp, precision="fp64", emi_precision="fp64", device=dev).run(rslc)
+        variants = precision_variants(cfg, rslc, ref, dev)
+        del ref
+        torch.cuda.empty_cache()
+    if not args.no_oracle and world == 1:
+        log("oracle check of the headline results")
+        oracle = oracle_check(cfg, rslc, res, args.precision, n_points=args.oracle_points)
+        log(f"oracle check: {oracle['frac_within_1mrad']} within 1 mrad, max {oracle['phase_err_max_rad']:.2e}")
 
     # rooflines: every stage against its bound; the headline is the dominant stage
     peaks = measured_peaks()
@@ -592,9 +678,9 @@ def main():
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": DTYPE[args.precision], "data": "synthetic",
+            "vs_baseline": None, "dtype": dtype_of(args.precision, chain.emi_precision), "data": "synthetic",
             "config": workload, "n_ds_per_gpu": n_ds, "stage_ms": stage, "roofline": roofline,
-            "stage_roofline": stage_roof, "precision_variants": variants,
+            "stage_roofline": stage_roof, "precision_variants": variants, "oracle_check": oracle,
             "cpu_baseline": cpu, "e2e": e2e, "scene_stream": stream, "latency": latency, "clocks": clk, "gpu_launches": launches,
         }))
     if world > 1:

@@ -54,6 +54,10 @@ enum {
   MR_PREC_FP64 = 3,   /* FP64 Gram; FP64 EMI */
   MR_PREC_MIXED = 4,  /* EMI only: FP32, with points whose cond_1(|Gamma|) estimate exceeds
                          the threshold (or that are singular in FP32) redone in FP64 */
+  MR_PREC_REFINE = 5, /* EMI only: inv(|Gamma|) in FP64, the Householder reduction in FP32,
+                         the eigenvector refined by one FP64 Newton step through the FP32
+                         factors, then checked in FP64; points whose phase error bound exceeds
+                         the tolerance (MR_EMI_REFINE_TOL) are redone in FP64 */
 };
 
 /* What the whole chain feeds the KS test (the test depends only on ranks, but the two
@@ -65,6 +69,8 @@ enum {
 
 /* Condition threshold of MR_PREC_MIXED in mr_emi. */
 #define MR_EMI_COND_MAX 1.0e4
+/* Phase error bound (rad) under which MR_PREC_REFINE keeps a refined point in mr_emi. */
+#define MR_EMI_REFINE_TOL 1.0e-4
 
 /* Limits of this build. */
 #define MR_MAX_NIMAGES 512
@@ -103,10 +109,13 @@ int mr_ks_test(const float* rmli, int nlines, int width, int nimages, int az_hal
 /* Replaces moraine.shp.select_shp (moraine/shp.py:309-323): is_shp = p < p_max (p
  * widened to double; NaN gives 0), shp_num = per-pixel count. */
 /* Tile plans of the KS merge: with autotuning on (off by default), the first mr_ks_test for a
- * (device, nimages, window) times the plans for several shared-memory budgets on its own
- * input (synchronising the stream; never inside a stream capture) and keeps the fastest;
- * results do not depend on the plan. mr_ks_plan reports the plan in use. No reference
- * counterpart (the reference kernel has no tiles). */
+ * (device, nimages, window, raster size within a factor of 4) times the plans for several
+ * shared-memory budgets on its own input, three times each (synchronising the stream; never
+ * inside a stream capture), and keeps the one with the fastest median; results do not depend
+ * on the plan. Timings are most reliable when nothing else runs on the device, e.g. in a
+ * first call before a server starts its slots. mr_ks_plan reports the plan in use (for the
+ * largest raster size tuned so far). No reference counterpart (the reference kernel has no
+ * tiles). */
 void mr_set_autotune(int on);
 int mr_ks_plan(int nimages, int az_half_win, int r_half_win, int* tile_rows, int* tile_cols,
                int* az_chunk);
@@ -134,10 +143,11 @@ int mr_ds_extract(const int32_t* shp_num, const uint8_t* is_shp, int nlines, int
  * and results as mr_ds_extract without the workspace: the per-block counts live in a
  * fixed array inside the library (128 KiB per device, held until the process exits), so
  * rasters are limited to MR_DS_EXTRACT_NOALLOC_MAX_PIXELS pixels (larger ones return
- * MR_ERR_UNSUPPORTED). It calls no allocator. The first call on a device looks up that
- * array's device address (cudaGetSymbolAddress); make that first call before any stream
- * capture. Every call shares the one array: calls that overlap on the GPU (other streams,
- * other host threads) race on it, so serialise them. */
+ * MR_ERR_UNSUPPORTED). It calls no allocator. The first call in a CUDA context looks up
+ * that array's device address (cudaGetSymbolAddress) and keeps it with the context's ID
+ * (a context created again after cudaDeviceReset gets a new lookup); make that first call
+ * before any stream capture. Every call shares the one array: calls that overlap on the
+ * GPU (other streams, other host threads) race on it, so serialise them. */
 #define MR_DS_EXTRACT_NOALLOC_MAX_PIXELS (16384LL * 1024LL)
 int mr_ds_extract_noalloc(const int32_t* shp_num, const uint8_t* is_shp, int nlines, int width,
                           int win, int min_shp, int32_t* idx, uint8_t* pc_is_shp, int64_t max_ds,
@@ -223,9 +233,10 @@ int mr_gamma_decode(const void* be, int64_t n, int dtype, void* out, int64_t out
  * algebraically smallest eigenpair (lambda, v), ph = v conj(v[ref]) / |v conj(v[ref])|,
  * emi_quality = lambda. inv(|Gamma|) by Gauss-Jordan with partial pivoting; eigenpair by
  * Householder tridiagonalisation, Sturm multisection and inverse iteration; all in the
- * arithmetic given by precision: MR_PREC_FP32, MR_PREC_FP64, or MR_PREC_MIXED (FP32, and
- * FP64 for the points whose cond_1(|Gamma|) estimate exceeds MR_EMI_COND_MAX); FP64
- * throughout when nimages > 128. t_coh (may be NULL) receives moraine.pl.ds_temp_coh of
+ * arithmetic given by precision: MR_PREC_FP32, MR_PREC_FP64, MR_PREC_MIXED (FP32, and
+ * FP64 for the points whose cond_1(|Gamma|) estimate exceeds MR_EMI_COND_MAX) or
+ * MR_PREC_REFINE (see mr_emi_refined, tolerance MR_EMI_REFINE_TOL); FP64 throughout when
+ * nimages > 128. t_coh (may be NULL) receives moraine.pl.ds_temp_coh of
  * the result (moraine/pl.py:126) computed in the same pass. Points whose |Gamma| is
  * singular at the arithmetic used get NaN (the reference's inv raises on them).
  * workspace: >= mr_emi_workspace_bytes() (the same for every precision). */
@@ -244,6 +255,21 @@ int mr_emi(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, int prec
 int mr_emi_routed(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, double cond_max,
                   mr_complex64* ph, float* emi_quality, float* t_coh, uint8_t* route,
                   void* workspace, size_t workspace_bytes, mr_stream_t stream);
+
+/* mr_emi with MR_PREC_REFINE and a caller-chosen tolerance tol (> 0, radians). inv(|Gamma|)
+ * is computed in FP64 and M = inv(|Gamma|) o Gamma is reduced to tridiagonal form in FP32.
+ * The FP32 eigenvector v is then improved by one Newton (Jacobi-Davidson) step in FP64:
+ * r = M v - lambda v with M and lambda = v^H M v in FP64, the correction solved through the
+ * FP32 factors M ~ Q T Q^H with T's own eigenvector projected out. The refined pair is
+ * checked in FP64: residual r', gap g = lambda_2(T) - lambda and smallest component
+ * min|v_i| bound the phase error of every date by |r'| / (g min|v_i|); points whose
+ * bound exceeds tol are recomputed in FP64. route (may be NULL, n_pc bytes) receives per
+ * point 0 = refined, 1 = recomputed in FP64, 2 = |Gamma| singular in FP64 (NaN output);
+ * 1 for every point when nimages > 128 (FP64 throughout). Same computation as
+ * moraine.pl.emi (moraine/pl.py:68-77); the refinement has no reference counterpart. */
+int mr_emi_refined(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, double tol,
+                   mr_complex64* ph, float* emi_quality, float* t_coh, uint8_t* route,
+                   void* workspace, size_t workspace_bytes, mr_stream_t stream);
 
 /* ---------------------------------------------------------------- raster <-> point cloud
  * Replace moraine.pc.ras2pc (moraine/pc.py:239-241: pc = ras[gix[:, 0], gix[:, 1]]) and
@@ -267,8 +293,9 @@ int mr_pc2ras(const void* pc, const int32_t* gix, int64_t n, int64_t nlines, int
  * moraine/cli/pl.py:223 (emi, ds_temp_coh) for one tile in device memory:
  * KS input (ks_input: MR_KS_INTENSITY or MR_KS_AMPLITUDE) -> KS test + SHP selection
  * (window (2 az_half_win + 1) x (2 r_half_win + 1), p < p_max) -> DS points (SHP count
- * >= min_shp, row-major order) -> per batch of at most `batch` points: coherence (gram_precision) -> EMI with temporal coherence (emi_precision:
- * MR_PREC_FP32, MR_PREC_FP64 or MR_PREC_MIXED). Outputs for the first *n_ds points: idx
+ * >= min_shp, row-major order) -> per batch of at most `batch` points: coherence
+ * (gram_precision) -> EMI with temporal coherence (emi_precision: MR_PREC_FP32,
+ * MR_PREC_FP64, MR_PREC_MIXED or MR_PREC_REFINE). Outputs for the first *n_ds points: idx
  * (max_ds, 2), ph (max_ds, nimages), quality and t_coh (max_ds). *n_ds is a host pointer:
  * the call synchronises `stream` once to read the DS count (fails with MR_ERR_INVALID when
  * it exceeds max_ds). workspace: >= mr_ds_chain_workspace_bytes(), 256-byte aligned. */

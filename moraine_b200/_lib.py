@@ -18,7 +18,7 @@ MR_ERR_CUDA = -2
 MR_ERR_UNSUPPORTED = -3
 MR_ERR_WORKSPACE = -4
 
-PREC = {"fp32": 0, "bf16": 1, "bf16x3": 2, "fp64": 3, "mixed": 4}
+PREC = {"fp32": 0, "bf16": 1, "bf16x3": 2, "fp64": 3, "mixed": 4, "refine": 5}
 KS_INPUT = {"intensity": 0, "amplitude": 1}
 
 MAX_NIMAGES = 512
@@ -60,6 +60,7 @@ _SIGNATURES = {
     "mr_emi_workspace_bytes": (c_size_t, [c_int64, c_int]),
     "mr_emi": (c_int, [P, c_int64, c_int, c_int, c_int, P, P, P, P, c_size_t, P]),
     "mr_emi_routed": (c_int, [P, c_int64, c_int, c_int, c_double, P, P, P, P, P, c_size_t, P]),
+    "mr_emi_refined": (c_int, [P, c_int64, c_int, c_int, c_double, P, P, P, P, P, c_size_t, P]),
     "mr_ds_temp_coh": (c_int, [P, P, c_int64, c_int, P, c_int, P, P]),
     "mr_temp_coh": (c_int, [P, P, c_int64, c_int, P, c_int, P, P]),
 }

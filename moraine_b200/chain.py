@@ -34,7 +34,7 @@ class ChainResult:
     shp_num: torch.Tensor | None  # (nlines, width) int32 (None in graph mode)
     is_shp: torch.Tensor | None   # (nlines, width, az_win, r_win) uint8 (None in graph mode)
     stage_ms: dict = field(default_factory=dict)
-    route: torch.Tensor | None = None  # (n_ds,) uint8 EMI route with emi_precision="mixed"
+    route: torch.Tensor | None = None  # (n_ds,) uint8 EMI route with emi_precision "mixed" or "refine"
 
 
 class DsChain:
@@ -43,7 +43,8 @@ class DsChain:
     def __init__(self, nlines: int, width: int, nimages: int, az_half_win: int, r_half_win: int,
                  p_max: float = 0.05, min_shp: int = 50, precision: str = "fp32", batch: int | None = None,
                  device=None, timing: bool = False, emi_precision: str | None = None,
-                 cond_max: float = 1.0e4, graph: bool = False, ks_input: str = "intensity"):
+                 cond_max: float = 1.0e4, graph: bool = False, ks_input: str = "intensity",
+                 refine_tol: float = 1.0e-4):
         self.device = torch.device(device) if device is not None else _dev.require_cuda()
         if ks_input not in _lib.KS_INPUT:
             raise ValueError(f"ks_input must be 'intensity' or 'amplitude', not {ks_input!r}")
@@ -59,11 +60,12 @@ class DsChain:
         # points to FP64
         if emi_precision is None:
             emi_precision = "fp64" if precision == "fp64" else "fp32"
-        if emi_precision not in ("fp32", "fp64", "mixed"):
-            raise ValueError(f"emi_precision must be 'fp32', 'fp64' or 'mixed', not {emi_precision!r}")
+        if emi_precision not in ("fp32", "fp64", "mixed", "refine"):
+            raise ValueError(f"emi_precision must be 'fp32', 'fp64', 'mixed' or 'refine', not {emi_precision!r}")
         self.emi_precision = emi_precision
         self.emi_prec = _lib.PREC[emi_precision]
         self.cond_max = float(cond_max)
+        self.refine_tol = float(refine_tol)
         self.timing = timing
         self.npairs = nimages * (nimages - 1) // 2
         npix = nlines * width
@@ -82,7 +84,8 @@ class DsChain:
         self.ph = torch.empty((npix, nimages), dtype=torch.complex64, device=d)
         self.quality = torch.empty((npix,), dtype=torch.float32, device=d)
         self.t_coh = torch.empty((npix,), dtype=torch.float32, device=d)
-        self.route = torch.empty((npix,), dtype=torch.uint8, device=d) if emi_precision == "mixed" else None
+        self.route = (torch.empty((npix,), dtype=torch.uint8, device=d) if emi_precision in ("mixed", "refine")
+                      else None)
         # CUDA-graph mode: the whole chain (mr_ds_chain_async, the DS count kept on the device)
         # captured once and replayed for every stack copied into a static input buffer
         self.graph = bool(graph)
@@ -186,7 +189,11 @@ class DsChain:
                       self.is_shp.data_ptr(), 1, self.az_win, self.r_win, None, self.npairs, self.coh.data_ptr(),
                       self.prec, s)
             mark("coherence")
-            if self.route is not None:
+            if self.emi_precision == "refine":
+                _lib.call("mr_emi_refined", self.coh.data_ptr(), nb, n, 0, self.refine_tol, self.ph[b0].data_ptr(),
+                          self.quality[b0:].data_ptr(), self.t_coh[b0:].data_ptr(), self.route[b0:].data_ptr(),
+                          self.emi_ws.data_ptr(), self.emi_ws.numel(), s)
+            elif self.route is not None:
                 _lib.call("mr_emi_routed", self.coh.data_ptr(), nb, n, 0, self.cond_max, self.ph[b0].data_ptr(),
                           self.quality[b0:].data_ptr(), self.t_coh[b0:].data_ptr(), self.route[b0:].data_ptr(),
                           self.emi_ws.data_ptr(), self.emi_ws.numel(), s)

@@ -77,8 +77,9 @@ extern "C" int mr_ds_chain(const mr_complex64* rslc, int nlines, int width, int 
   MR_REQUIRE(nlines > 0 && width > 0 && nimages >= 2, "ds_chain: bad stack shape");
   MR_REQUIRE(az_half_win >= 0 && r_half_win >= 0, "ds_chain: negative half window");
   MR_REQUIRE(batch > 0 && max_ds >= 0, "ds_chain: batch must be > 0 and max_ds >= 0");
-  MR_REQUIRE(emi_precision == MR_PREC_FP32 || emi_precision == MR_PREC_FP64 || emi_precision == MR_PREC_MIXED,
-             "ds_chain: emi_precision must be FP32, FP64 or MIXED");
+  MR_REQUIRE(emi_precision == MR_PREC_FP32 || emi_precision == MR_PREC_FP64 || emi_precision == MR_PREC_MIXED ||
+                 emi_precision == MR_PREC_REFINE,
+             "ds_chain: emi_precision must be FP32, FP64, MIXED or REFINE");
   const int az_win = 2 * az_half_win + 1, r_win = 2 * r_half_win + 1, win = az_win * r_win;
   const size_t need = mr_ds_chain_workspace_bytes(nlines, width, nimages, az_half_win, r_half_win, batch);
   if (!workspace || workspace_bytes < need)

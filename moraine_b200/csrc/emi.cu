@@ -236,9 +236,10 @@ int emi_entry(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, int p
   if (nimages > MR_MAX_NIMAGES) return fail(MR_ERR_UNSUPPORTED, "emi: nimages %d > %d", nimages, MR_MAX_NIMAGES);
   MR_REQUIRE(ref >= 0 && ref < nimages, "emi: ref %d out of range [0, %d)", ref, nimages);
   MR_REQUIRE(n_pc >= 0, "emi: negative n_pc");
-  MR_REQUIRE(precision == MR_PREC_FP32 || precision == MR_PREC_FP64 || precision == MR_PREC_MIXED,
-             "emi: precision must be FP32, FP64 or MIXED");
-  MR_REQUIRE(cond_max > 0, "emi: cond_max must be positive");
+  MR_REQUIRE(precision == MR_PREC_FP32 || precision == MR_PREC_FP64 || precision == MR_PREC_MIXED ||
+                 precision == MR_PREC_REFINE,
+             "emi: precision must be FP32, FP64, MIXED or REFINE");
+  MR_REQUIRE(cond_max > 0, "emi: cond_max (or the refinement tolerance) must be positive");
   if (n_pc == 0) return MR_OK;
   MR_REQUIRE(coh && ph && emi_quality, "emi: NULL pointer");
   const size_t need = mr_emi_workspace_bytes(n_pc, nimages);
@@ -266,7 +267,15 @@ int emi_entry(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, int p
 extern "C" int mr_emi(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, int precision,
                       mr_complex64* ph, float* emi_quality, float* t_coh, void* workspace, size_t workspace_bytes,
                       mr_stream_t stream) {
-  return emi_entry(coh, n_pc, nimages, ref, precision, MR_EMI_COND_MAX, ph, emi_quality, t_coh, nullptr, workspace,
+  return emi_entry(coh, n_pc, nimages, ref, precision,
+                   precision == MR_PREC_REFINE ? MR_EMI_REFINE_TOL : MR_EMI_COND_MAX, ph, emi_quality, t_coh,
+                   nullptr, workspace, workspace_bytes, stream);
+}
+
+extern "C" int mr_emi_refined(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, double tol,
+                              mr_complex64* ph, float* emi_quality, float* t_coh, uint8_t* route, void* workspace,
+                              size_t workspace_bytes, mr_stream_t stream) {
+  return emi_entry(coh, n_pc, nimages, ref, MR_PREC_REFINE, tol, ph, emi_quality, t_coh, route, workspace,
                    workspace_bytes, stream);
 }
 

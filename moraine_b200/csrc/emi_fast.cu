@@ -40,8 +40,9 @@ struct GjGrid {
 
 template <typename T, int NB, int CX>
 struct GjShared {
-  T col[2][16 * NB];
-  int piv[2];
+  T col[2][16 * NB];  // pivot column of the next step, by step parity
+  T rp[2];            // its pivot's reciprocal
+  int piv[2];         // its pivot row
   int piv_of_step[16 * NB];
   int step_of_row[16 * NB];
   T part[GjGrid<NB, CX>::kWarps][16 * NB];  // row sums of |a| per warp (norm estimate)
@@ -108,39 +109,60 @@ __device__ __forceinline__ void load_abs_gamma(T (&a)[NB][GjGrid<NB, CX>::NC], u
 __device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double recip(double x) { return __drcp_rn(x); }  // = 1.0 / x, IEEE round-to-nearest
 
+// Pivot search key of candidate row `row` (< 128) with value v: the largest key is the row
+// with the largest |v| to 15 bits of mantissa (ties to the smaller row); NaN ranks below
+// every number and above the rows already used (key 0).
+template <typename T> __device__ __forceinline__ unsigned pivot_key(T v, int row, bool eligible) {
+  const float a = fabsf((float)v);
+  const unsigned hi = (a == a) ? (__float_as_uint(a) >> 8) + 1u : 0u;
+  return eligible ? (hi << 8) | 128u | (127u - (unsigned)row) : 0u;
+}
+
+// Bring column SLOT of the half-warp's register tile up to date (a -= f_i r, as the step
+// does everywhere) and publish it as the pivot column of the next step, with its pivot
+// (largest |a| among the rows not used yet) and the pivot's reciprocal. Called by the 16
+// lanes of one column group; `col` holds f (the step's pivot column).
+template <typename T, int NB, int CX, int SLOT>
+__device__ __forceinline__ void gj_publish(T (&a)[NB][GjGrid<NB, CX>::NC], const T* col, T r, int p, T pv,
+                                           unsigned used, int ty, int buf, GjShared<T, NB, CX>& s) {
+  unsigned best = 0;
+#pragma unroll
+  for (int ib = 0; ib < NB; ++ib) {
+    const int i = ty + 16 * ib;
+    const T fi = (i == p) ? pv - T(1) : (col ? col[i] : T(0));
+    a[ib][SLOT] -= fi * r;
+    s.col[buf][i] = a[ib][SLOT];
+    best = max(best, pivot_key(a[ib][SLOT], i, !(used & (1u << ib))));
+  }
+  const unsigned half = (threadIdx.x & 16) ? 0xFFFF0000u : 0x0000FFFFu;
+  best = __reduce_max_sync(half, best);
+  const int p1 = min(127 - (int)(best & 127u), 16 * NB - 1);  // an unused row exists: best >= 128
+  if (ty == (p1 & 15)) {
+    T v = a[0][SLOT];
+#pragma unroll
+    for (int q = 1; q < NB; ++q) v = ((p1 >> 4) == q) ? a[q][SLOT] : v;
+    s.piv[buf] = p1;
+    s.rp[buf] = recip(v);
+  }
+}
+
 // One Gauss-Jordan step k = CX KB + kt on the register tile; KB is a compile-time column
 // slot, so the pivot column is read and rewritten without dynamic register indexing.
+// Look-ahead: the column group owning column k + 1 first brings that column up to date
+// and publishes it with its pivot and reciprocal (gj_publish), then does the rest of its
+// update; the step's other threads only read what the previous step published. One
+// barrier per step.
 template <typename T, int NB, int CX, int KB>
-__device__ __forceinline__ void gj_step(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned& used, int k, int tx, int ty,
-                                        bool& singular, GjShared<T, NB, CX>& s) {
+__device__ __forceinline__ void gj_step(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned& used, int k, int n, int tx,
+                                        int ty, bool& singular, GjShared<T, NB, CX>& s) {
   constexpr int NC = GjGrid<NB, CX>::NC;
+  constexpr int KB1 = KB + 1 < NC ? KB + 1 : 0;
   const int tid = threadIdx.x;
   const int buf = k & 1;
-  const bool owner = tx == (k % CX);
-  if (owner) {  // the half-warp owning column k: publish it, find the pivot
-    const unsigned half = (tx & 1) ? 0xFFFF0000u : 0x0000FFFFu;
-    T best = T(-1);
-    int bi = -1;
-#pragma unroll
-    for (int ib = 0; ib < NB; ++ib) {
-      const T v = a[ib][KB];
-      s.col[buf][ty + 16 * ib] = v;
-      const T av = fabs(v) == fabs(v) ? fabs(v) : T(-0.5);  // NaN ranks last but is taken
-      if (!(used & (1u << ib)) && av > best) { best = av; bi = ty + 16 * ib; }
-    }
-#pragma unroll
-    for (int o = 8; o > 0; o >>= 1) {
-      const T ob = __shfl_xor_sync(half, best, o, 16);
-      const int oi = __shfl_xor_sync(half, bi, o, 16);
-      if (ob > best || (ob == best && oi >= 0 && (bi < 0 || oi < bi))) { best = ob; bi = oi; }
-    }
-    if (ty == 0) s.piv[buf] = bi;
-  }
-  __syncthreads();
   const int p = s.piv[buf];
   T pv = s.col[buf][p];
-  if (pv == T(0)) { singular = true; pv = T(1); }
-  const T rp = recip(pv);
+  T rp = s.rp[buf];
+  if (pv == T(0)) { singular = true; pv = T(1); rp = T(1); }
   if (ty == (p & 15)) used |= 1u << (p >> 4);
   if (tid == 0) { s.piv_of_step[k] = p; s.step_of_row[p] = k; }
   const int pl = p & 15;
@@ -158,17 +180,30 @@ __device__ __forceinline__ void gj_step(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned
     default: MR_GJ_ROW(7)
 #undef MR_GJ_ROW
   }
-  // a -= f_i r_j everywhere, with f_p = pv - 1 so that the pivot row becomes r; then
-  // column k becomes delta_ip / pv - f_i / pv
+  // look-ahead: column k + 1 sits in slot KB of the next column group, or in slot KB + 1 of
+  // group 0 when k + 1 is a multiple of CX
+  const int k1 = k + 1;
+  const bool wrap = (k1 % CX) == 0;
+  const bool la = k1 < n && tx == k1 % CX && (!wrap || KB + 1 < NC);
+  const int la_slot = la ? (wrap ? KB1 : KB) : -1;
+  if (la) {
+    if (!wrap) gj_publish<T, NB, CX, KB>(a, s.col[buf], r[KB], p, pv, used, ty, buf ^ 1, s);
+    else gj_publish<T, NB, CX, KB1>(a, s.col[buf], r[KB1], p, pv, used, ty, buf ^ 1, s);
+  }
+  // a -= f_i r_j everywhere (the look-ahead column is done), with f_p = pv - 1 so that the
+  // pivot row becomes r; then column k becomes delta_ip / pv - f_i / pv
+  const bool owner = tx == (k % CX);
 #pragma unroll
   for (int ib = 0; ib < NB; ++ib) {
     const int i = ty + 16 * ib;
-    const T fi = s.col[buf][i];
-    const T f = (i == p) ? pv - T(1) : fi;
+    const T f = s.col[buf][i];
+    const T fi = (i == p) ? pv - T(1) : f;
 #pragma unroll
-    for (int jb = 0; jb < NC; ++jb) a[ib][jb] -= f * r[jb];
-    if (owner) a[ib][KB] = (i == p) ? rp : -fi * rp;
+    for (int jb = 0; jb < NC; ++jb)
+      if (jb != la_slot) a[ib][jb] -= fi * r[jb];
+    if (owner) a[ib][KB] = (i == p) ? rp : -f * rp;
   }
+  __syncthreads();
 }
 
 // In-place Gauss-Jordan inverse with partial pivoting on the register tile. Returns true
@@ -178,20 +213,23 @@ __device__ bool gj_tile(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned used, int n, in
                         GjShared<T, NB, CX>& s) {
   constexpr int NC = GjGrid<NB, CX>::NC;
   bool singular = false;
-#pragma unroll
+  // column 0 and its pivot, published by column group 0
+  if (tx == 0) gj_publish<T, NB, CX, 0>(a, nullptr, T(0), -1, T(1), used, ty, 0, s);
+  __syncthreads();
+#pragma unroll 1
   for (int kb = 0; kb < NC; ++kb) {
     for (int kt = 0; kt < CX; ++kt) {
       const int k = CX * kb + kt;
       if (k >= n) break;
-      switch (kb) {  // compile-time slot (the loop over kb is unrolled)
-        case 0: gj_step<T, NB, CX, 0>(a, used, k, tx, ty, singular, s); break;
-        case 1: if (NC > 1) gj_step<T, NB, CX, (1 < NC ? 1 : 0)>(a, used, k, tx, ty, singular, s); break;
-        case 2: if (NC > 2) gj_step<T, NB, CX, (2 < NC ? 2 : 0)>(a, used, k, tx, ty, singular, s); break;
-        case 3: if (NC > 3) gj_step<T, NB, CX, (3 < NC ? 3 : 0)>(a, used, k, tx, ty, singular, s); break;
-        case 4: if (NC > 4) gj_step<T, NB, CX, (4 < NC ? 4 : 0)>(a, used, k, tx, ty, singular, s); break;
-        case 5: if (NC > 5) gj_step<T, NB, CX, (5 < NC ? 5 : 0)>(a, used, k, tx, ty, singular, s); break;
-        case 6: if (NC > 6) gj_step<T, NB, CX, (6 < NC ? 6 : 0)>(a, used, k, tx, ty, singular, s); break;
-        default: if (NC > 7) gj_step<T, NB, CX, (7 < NC ? 7 : 0)>(a, used, k, tx, ty, singular, s); break;
+      switch (kb) {  // compile-time slot for each kb
+        case 0: gj_step<T, NB, CX, 0>(a, used, k, n, tx, ty, singular, s); break;
+        case 1: if (NC > 1) gj_step<T, NB, CX, (1 < NC ? 1 : 0)>(a, used, k, n, tx, ty, singular, s); break;
+        case 2: if (NC > 2) gj_step<T, NB, CX, (2 < NC ? 2 : 0)>(a, used, k, n, tx, ty, singular, s); break;
+        case 3: if (NC > 3) gj_step<T, NB, CX, (3 < NC ? 3 : 0)>(a, used, k, n, tx, ty, singular, s); break;
+        case 4: if (NC > 4) gj_step<T, NB, CX, (4 < NC ? 4 : 0)>(a, used, k, n, tx, ty, singular, s); break;
+        case 5: if (NC > 5) gj_step<T, NB, CX, (5 < NC ? 5 : 0)>(a, used, k, n, tx, ty, singular, s); break;
+        case 6: if (NC > 6) gj_step<T, NB, CX, (6 < NC ? 6 : 0)>(a, used, k, n, tx, ty, singular, s); break;
+        default: if (NC > 7) gj_step<T, NB, CX, (7 < NC ? 7 : 0)>(a, used, k, n, tx, ty, singular, s); break;
       }
     }
   }
@@ -200,24 +238,24 @@ __device__ bool gj_tile(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned used, int n, in
 }
 
 // ----------------------------------------------------------------- packed reduction
+// Shared memory of the reduction (n = nimages):
+//   L    packed lower triangle of M by rows, (i, j <= i) at tri(i) + j
+//   vec  [2][n] reflectors u_k and u_{k-1}, by step parity
+//   wp   [n]    w_{k-1} of the pending rank-2 update
+//   rowp [n]    row part of the product of the last step, one value per row
+//   cp   [kWarps][n] column part of that product, one partial per warp
+//   d, tau [n], e [n] the tridiagonal and the reflector scalars
 template <typename T>
 struct TriShared {
   using C = typename C2<T>::type;
-  C* L;       // lower triangle, packed by rows: (i, j <= i) at i(i+1)/2 + j
-  C* pv;      // [2][n] products of the last two steps
-  C* vec;     // [3][n]: u_k and u_{k-1} (by step parity), w_{k-1}
+  C* L;
+  C* vec;
+  C* wp;
+  C* rowp;
+  C* cp;
   C* e;
-  C* z;
-  double2* phs;
   T* d;
   T* tau;
-  T* b;
-  T* b2;
-  T* y;
-  T* w1;
-  T* w2;
-  T* w3;
-  Red* red;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -227,40 +265,24 @@ template <typename T>
 __host__ __device__ inline size_t tri_bytes(int n) {
   using C = typename C2<T>::type;
   size_t o = align16((size_t)n * (n + 1) / 2 * sizeof(C));
-  o = align16(o + 2 * (size_t)n * sizeof(C));
-  o = align16(o + 3 * (size_t)n * sizeof(C));
-  o = align16(o + 2 * (size_t)n * sizeof(C));
-  o = align16(o + (size_t)n * sizeof(double2));
-  o = align16(o + 8 * (size_t)n * sizeof(T));
-  return o + sizeof(Red);
+  o += align16((size_t)(2 + 1 + 1 + kWarps + 1) * n * sizeof(C));
+  o += align16(2 * (size_t)n * sizeof(T));
+  return o;
 }
 
 template <typename T>
 __device__ inline TriShared<T> tri_layout(unsigned char* base, int n) {
   using C = typename C2<T>::type;
   TriShared<T> s;
-  size_t o = 0;
-  s.L = reinterpret_cast<C*>(base + o);
-  o = align16(o + (size_t)n * (n + 1) / 2 * sizeof(C));
-  s.pv = reinterpret_cast<C*>(base + o);
-  o = align16(o + 2 * (size_t)n * sizeof(C));
-  s.vec = reinterpret_cast<C*>(base + o);
-  o = align16(o + 3 * (size_t)n * sizeof(C));
-  s.e = reinterpret_cast<C*>(base + o);
-  s.z = s.e + n;
-  o = align16(o + 2 * (size_t)n * sizeof(C));
-  s.phs = reinterpret_cast<double2*>(base + o);
-  o = align16(o + (size_t)n * sizeof(double2));
-  s.d = reinterpret_cast<T*>(base + o);
+  s.L = reinterpret_cast<C*>(base);
+  C* v = reinterpret_cast<C*>(base + align16((size_t)n * (n + 1) / 2 * sizeof(C)));
+  s.vec = v;
+  s.wp = v + 2 * n;
+  s.rowp = v + 3 * n;
+  s.cp = v + 4 * n;
+  s.e = v + (4 + kWarps) * n;
+  s.d = reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(v) + align16((size_t)(5 + kWarps) * n * sizeof(C)));
   s.tau = s.d + n;
-  s.b = s.tau + n;
-  s.b2 = s.b + n;
-  s.y = s.b2 + n;
-  s.w1 = s.y + n;
-  s.w2 = s.w1 + n;
-  s.w3 = s.w2 + n;
-  o = align16(o + 8 * (size_t)n * sizeof(T));
-  s.red = reinterpret_cast<Red*>(base + o);
   return s;
 }
 
@@ -269,47 +291,93 @@ template <typename C> __device__ __forceinline__ void rank2(C& a, C ui, C wj, C 
   a.x -= ui.x * wj.x + ui.y * wj.y + wi.x * uj.x + wi.y * uj.y;
   a.y -= ui.y * wj.x - ui.x * wj.y + wi.y * uj.x - wi.x * uj.y;
 }
+// acc += a b
+template <typename C> __device__ __forceinline__ void cmac(C& acc, C a, C b) {
+  acc.x += a.x * b.x - a.y * b.y;
+  acc.y += a.x * b.y + a.y * b.x;
+}
+// acc += conj(a) b
+template <typename C> __device__ __forceinline__ void cmacc(C& acc, C a, C b) {
+  acc.x += a.x * b.x + a.y * b.y;
+  acc.y += a.x * b.y - a.y * b.x;
+}
+template <typename C> __device__ __forceinline__ C shfl_xor_c(C v, int o) {
+  v.x = __shfl_xor_sync(0xffffffffu, v.x, o);
+  v.y = __shfl_xor_sync(0xffffffffu, v.y, o);
+  return v;
+}
+
+// Sum over the 32 lanes of four per-lane values r[0..3] (reduce-scatter): afterwards lane l
+// holds the total of value (l >> 3) & 3 (lanes 0, 8, 16, 24 hold values 0, 1, 2, 3).
+template <typename C> __device__ __forceinline__ C warp_sum4(const C (&r)[4]) {
+  const int lane = threadIdx.x & 31;
+  const bool hi4 = lane & 16, hi3 = lane & 8;
+  C k0 = hi4 ? r[2] : r[0], k1 = hi4 ? r[3] : r[1];
+  const C s0 = hi4 ? r[0] : r[2], s1 = hi4 ? r[1] : r[3];
+  k0 = cadd(k0, shfl_xor_c(s0, 16));
+  k1 = cadd(k1, shfl_xor_c(s1, 16));
+  C k = hi3 ? k1 : k0;
+  k = cadd(k, shfl_xor_c(hi3 ? k0 : k1, 8));
+  k = cadd(k, shfl_xor_c(k, 4));
+  k = cadd(k, shfl_xor_c(k, 2));
+  k = cadd(k, shfl_xor_c(k, 1));
+  return k;
+}
+
+// Product of the last step for row i: rowp[i] + sum of the warps' column partials.
+template <typename T>
+__device__ __forceinline__ typename C2<T>::type prod_of(const TriShared<T>& s, int n, int i) {
+  typename C2<T>::type p = s.rowp[i];
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) p = cadd(p, s.cp[w * n + i]);
+  return p;
+}
 
 // Householder reduction of the Hermitian M (lower triangle, packed in s.L) to tridiagonal
-// (s.d, s.e); reflector k stored in column k (rows k+1..n-1) with scalar s.tau[k]. Whole
-// CTA, three barriers per step:
-//   1. warp 0 finishes step k-1 (w = p - K u, K = tau/2 u^H p) and forms reflector k from
-//      column k brought up to date, x_i = A_i + K B_i, with A_i and B_i computed in the same
-//      pass as the dot product (one load pass, two warp reductions);
-//   2. phase 1: step k-1's rank-2 update on the lower triangle of rows >= k+1 and the row
-//      part of (M u_k)_i = sum_{j<=i} M_ij u_j;
-//   3. phase 2: the column part sum_{j>i} conj(M_ji) u_j, then p_k = tau_k M u_k.
-// Rows are handled in mirrored pairs (i, n+k-i) by groups of 4 to 32 threads (as many as
-// keep the CTA busy while the trailing matrix shrinks), which gives every thread of a step
-// the same number of elements in both phases. The packed triangle halves the
-// shared memory of full storage, so twice as many points are in flight per SM.
+// (s.d, s.e); reflector k is left in column k (rows k+1..n-1) with scalar s.tau[k]. The
+// whole CTA, two barriers per step k:
+//   S (warp 0): finish step k-1 (p = tau M u, K = tau/2 u^H p, w = p - K u) and form
+//     reflector k from column k with step k-1's update applied on the fly,
+//     x_i = A_i + K B_i, A_i and B_i from the same loads as the dot product;
+//   P (all warps): one pass over the trailing triangle (rows and columns k+1..n-1). Each
+//     element is loaded once: step k-1's rank-2 update is applied and stored, and the
+//     element adds to both products it takes part in, row i (M_ij u_j) and column j
+//     (conj(M_ij) u_i). A warp takes one row at a time with its lanes over the columns,
+//     rows in mirrored pairs so that every warp has the same count of elements; row sums
+//     are reduce-scattered four rows at a time, column sums stay in the lanes and are
+//     written once per warp. The S warp adds the partials in a fixed order, so results
+//     do not depend on timing.
 template <typename T>
 __device__ void tridiag_packed(const TriShared<T>& s, int n) {
   using C = typename C2<T>::type;
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  constexpr int NC = (kMaxFastN + 31) / 32;  // column slots of a lane
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   C* L = s.L;
-  C* wp = s.vec + 2 * n;  // w_{k-1}
   for (int k = 0; k + 2 < n; ++k) {
     C* up = s.vec + ((k + 1) & 1) * n;  // u_{k-1}
     C* uc = s.vec + (k & 1) * n;        // u_k
-    // ---- warp 0: finish step k-1 and form reflector k
+    // ---- S: warp 0 finishes step k-1 and forms reflector k
     if (wid == 0) {
       const T tau_prev = k > 0 ? s.tau[k - 1] : T(0);
       const bool pending = tau_prev != T(0);
-      const C* p = s.pv + ((k + 1) & 1) * n;
-      C A[4], B[4], pp[4], uu[4];
+      C A[NC], B[NC], pp[NC], uu[NC];
       T dot = 0;
       C pk = mk<T>(0, 0), ukk = mk<T>(0, 0);
-      if (pending) { pk = p[k]; ukk = up[k]; }
+      if (pending) {
+        pk = prod_of(s, n, k);
+        pk = mk<T>(tau_prev * pk.x, tau_prev * pk.y);
+        ukk = up[k];
+      }
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
+      for (int t = 0; t < NC; ++t) {
         const int i = k + lane + 32 * t;
         A[t] = B[t] = pp[t] = uu[t] = mk<T>(0, 0);
         if (i < n) {
           const int base = tri(i);
           A[t] = L[base + k];
           if (pending) {
-            pp[t] = p[i];
+            const C q = prod_of(s, n, i);
+            pp[t] = mk<T>(tau_prev * q.x, tau_prev * q.y);
             uu[t] = up[i];
             dot += uu[t].x * pp[t].x + uu[t].y * pp[t].y;
             // x_i = a_ik - u_i conj(w_k) - w_i conj(u_k) = A_i + K B_i, w = p - K u
@@ -322,11 +390,11 @@ __device__ void tridiag_packed(const TriShared<T>& s, int n) {
       const T K = pending ? T(0.5) * tau_prev * warp_sum(dot) : T(0);
       T xn2 = 0;
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
+      for (int t = 0; t < NC; ++t) {
         const int i = k + lane + 32 * t;
         if (i < n) {
           const C x = mk<T>(A[t].x + K * B[t].x, A[t].y + K * B[t].y);
-          if (pending) wp[i] = mk<T>(pp[t].x - K * uu[t].x, pp[t].y - K * uu[t].y);
+          if (pending) s.wp[i] = mk<T>(pp[t].x - K * uu[t].x, pp[t].y - K * uu[t].y);
           uc[i] = x;
           if (i >= k + 2) xn2 += x.x * x.x + x.y * x.y;
         }
@@ -347,58 +415,74 @@ __device__ void tridiag_packed(const TriShared<T>& s, int n) {
       if (lane == 0) { s.d[k] = uc[k].x; s.e[k] = ek; s.tau[k] = tau_k; }
     }
     __syncthreads();
+    // ---- P: step k-1's update and the product M u_k over rows/columns k+1..n-1
     const bool pending = k > 0 && s.tau[k - 1] != T(0);
-    const T tau_k = s.tau[k];
-    const int m = n - k - 1;         // rows k+1..n-1
-    const int npair = (m + 1) >> 1;  // mirrored pairs (the middle row of an odd m alone)
-    // G threads per pair, as many as keep every thread of the CTA busy (4 to 32)
-    int G = 4;
-    while (G < 32 && npair * G * 2 <= (int)blockDim.x) G <<= 1;
-    const int pq = tid / G, sub = tid & (G - 1);
-    const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u) << (lane & ~(G - 1));
-    const bool active = (pending || tau_k != T(0)) && pq < npair;
-    const int i1 = k + 1 + pq, i2 = n - 1 - pq;
-    const bool two = i2 != i1;
-    // ---- phase 1: update the lower rows, row part of M u
-    C rs1 = mk<T>(0, 0), rs2 = mk<T>(0, 0);
-    if (active) {
-#pragma unroll 1
-      for (int r = 0; r < 2; ++r) {
-        if (r && !two) break;
-        const int i = r ? i2 : i1;
-        C* row = L + tri(i);
-        C upi = mk<T>(0, 0), wpi = mk<T>(0, 0);
-        if (pending) { upi = up[i]; wpi = wp[i]; }
-        C acc = mk<T>(0, 0);
-        for (int j = k + 1 + sub; j <= i; j += G) {
-          C a = row[j];
-          if (pending) { rank2(a, upi, wp[j], wpi, up[j]); row[j] = a; }
-          const C u = uc[j];
-          acc.x += a.x * u.x - a.y * u.y;
-          acc.y += a.x * u.y + a.y * u.x;
-        }
-        if (r) rs2 = acc; else rs1 = acc;
+    const bool mv = s.tau[k] != T(0);
+    if (!pending && !mv) continue;  // CTA-uniform; nothing reads this step's product
+    const int k1 = k + 1;
+    const int m = n - k1;
+    C ui[NC], upi[NC], wpi[NC], cacc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const int i = k1 + lane + 32 * c;
+      ui[c] = upi[c] = wpi[c] = cacc[c] = mk<T>(0, 0);
+      if (i < n) {
+        ui[c] = uc[i];
+        if (pending) { upi[c] = up[i]; wpi[c] = s.wp[i]; }
       }
     }
-    __syncthreads();
-    // ---- phase 2: column part, then p_k
-    if (active && tau_k != T(0)) {
-#pragma unroll 1
-      for (int r = 0; r < 2; ++r) {
-        if (r && !two) break;
-        const int i = r ? i2 : i1;
-        C acc = r ? rs2 : rs1;
-        for (int j = i + 1 + sub; j < n; j += G) {
-          const C a = L[tri(j) + i];  // M_ji, lower triangle
-          const C u = uc[j];
-          acc.x += a.x * u.x + a.y * u.y;  // conj(M_ji) u_j
-          acc.y += a.x * u.y - a.y * u.x;
+    const int npair = (m + 1) >> 1;
+    for (int q0 = wid; q0 < npair; q0 += 2 * kWarps) {
+      // rows of this round: pair q0 and pair q0 + kWarps, each (k1 + q, n - 1 - q)
+      const bool two = q0 + kWarps < npair;
+      C racc[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        racc[r] = mk<T>(0, 0);
+        const int q = q0 + (r >> 1) * kWarps;
+        const int jj = (r & 1) ? n - 1 - q : k1 + q;
+        if ((r >> 1) && !two) continue;         // warp-uniform
+        if ((r & 1) && jj == k1 + q) continue;  // middle row of an odd count, taken once
+        const int base = tri(jj);
+        const C ucj = uc[jj];
+        C upj = mk<T>(0, 0), wpj = mk<T>(0, 0);
+        if (pending) { upj = up[jj]; wpj = s.wp[jj]; }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          if (k1 + 32 * c > jj) break;  // slot entirely right of the diagonal (warp-uniform)
+          const int i = k1 + lane + 32 * c;
+          if (i <= jj) {
+            C a = L[base + i];
+            if (pending) {
+              rank2(a, upj, wpi[c], wpj, upi[c]);
+              L[base + i] = a;
+            }
+            if (mv) {
+              if (i < jj) {
+                cmac(racc[r], a, ui[c]);
+                cmacc(cacc[c], a, ucj);
+              } else {
+                racc[r].x += a.x * ui[c].x;
+                racc[r].y += a.x * ui[c].y;
+              }
+            }
+          }
         }
-        for (int o = 1; o < G; o <<= 1) {
-          acc.x += __shfl_xor_sync(gmask, acc.x, o);
-          acc.y += __shfl_xor_sync(gmask, acc.y, o);
-        }
-        if (sub == 0) s.pv[(k & 1) * n + i] = mk<T>(tau_k * acc.x, tau_k * acc.y);
+      }
+      if (mv) {
+        const C tot = warp_sum4(racc);
+        const int r = lane >> 3;
+        const int q = q0 + (r >> 1) * kWarps;
+        const int jj = (r & 1) ? n - 1 - q : k1 + q;
+        const bool ok = (!(r >> 1) || two) && !((r & 1) && jj == k1 + q);
+        if ((lane & 7) == 0 && ok) s.rowp[jj] = tot;
+      }
+    }
+    if (mv) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const int i = k1 + lane + 32 * c;
+        if (i < n) s.cp[wid * n + i] = cacc[c];
       }
     }
     __syncthreads();
@@ -408,21 +492,23 @@ __device__ void tridiag_packed(const TriShared<T>& s, int n) {
     if (n >= 3 && s.tau[n - 3] != T(0)) {
       const T tau_prev = s.tau[n - 3];
       const C* up = s.vec + ((n - 3) & 1) * n;
-      const C* p = s.pv + ((n - 3) & 1) * n;
       T dot = 0;
-      for (int i = n - 2 + lane; i < n; i += 32) {
-        const C pi = p[i], ui = up[i];
-        wp[i] = pi;
-        dot += ui.x * pi.x + ui.y * pi.y;
+      C pi = mk<T>(0, 0), ui = mk<T>(0, 0);
+      const int i = n - 2 + lane;
+      if (lane < 2) {
+        const C q = prod_of(s, n, i);
+        pi = mk<T>(tau_prev * q.x, tau_prev * q.y);
+        ui = up[i];
+        dot = ui.x * pi.x + ui.y * pi.y;
       }
       const T K = T(0.5) * tau_prev * warp_sum(dot);
-      for (int i = n - 2 + lane; i < n; i += 32) { wp[i].x -= K * up[i].x; wp[i].y -= K * up[i].y; }
+      if (lane < 2) s.wp[i] = mk<T>(pi.x - K * ui.x, pi.y - K * ui.y);
       __syncwarp();
       if (lane < 3) {
-        const int i = (lane == 0) ? n - 2 : n - 1, j = (lane == 2) ? n - 1 : n - 2;
-        rank2(L[tri(i) + j], up[i], wp[j], wp[i], up[j]);
+        const int r = (lane == 0) ? n - 2 : n - 1, c = (lane == 2) ? n - 1 : n - 2;
+        rank2(L[tri(r) + c], up[r], s.wp[c], s.wp[r], up[c]);
       }
-      for (int i = n - 2 + lane; i < n; i += 32) L[tri(i) + n - 3] = up[i];
+      if (lane < 2) L[tri(i) + n - 3] = up[i];
       __syncwarp();
     }
     if (lane == 0) {
@@ -435,33 +521,39 @@ __device__ void tridiag_packed(const TriShared<T>& s, int n) {
 }
 
 // ----------------------------------------------------------------- workspace layout
-// Per point: inv(|Gamma|) lower triangle packed (np T), reflectors (column k rows
-// k+1..n-1, packed by column, nq complex T), d and tau (n T each), e (n complex T).
-template <typename T>
+// Per point: inv(|Gamma|) in the arithmetic TA of the inverse, packed upper triangle by
+// rows like the compressed coherence ((m, j >= m) at tri_up(m, j)); then, in the arithmetic
+// T of the reduction, the reflectors (column k rows k+1..n-1, packed by column, nq complex
+// T), d and tau (n T each), e (n complex T).
+__host__ __device__ __forceinline__ int64_t tri_up(int m, int j, int n) {
+  return (int64_t)m * n - ((int64_t)m * (m - 1)) / 2 + (j - m);
+}
+
+template <typename T, typename TA = T>
 struct PointWs {
   size_t np, nq, bytes;
   __host__ __device__ explicit PointWs(int n) {
     using C = typename C2<T>::type;
     np = (size_t)n * (n + 1) / 2;
     nq = (size_t)n * (n - 1) / 2;
-    bytes = align16(np * sizeof(T)) + align16(nq * sizeof(C)) + align16(2 * (size_t)n * sizeof(T)) +
+    bytes = align16(np * sizeof(TA)) + align16(nq * sizeof(C)) + align16(2 * (size_t)n * sizeof(T)) +
             align16((size_t)n * sizeof(C));
   }
 };
 
-template <typename T>
+template <typename T, typename TA = T>
 struct PointPtr {
   using C = typename C2<T>::type;
-  T* ainv;
+  TA* ainv;
   C* refl;
   T* d;
   T* tau;
   C* e;
   __device__ PointPtr(unsigned char* ws, int64_t pt, int n) {
-    const PointWs<T> w(n);
+    const PointWs<T, TA> w(n);
     unsigned char* b = ws + (size_t)pt * w.bytes;
-    ainv = reinterpret_cast<T*>(b);
-    b += align16(w.np * sizeof(T));
+    ainv = reinterpret_cast<TA*>(b);
+    b += align16(w.np * sizeof(TA));
     refl = reinterpret_cast<C*>(b);
     b += align16(w.nq * sizeof(C));
     d = reinterpret_cast<T*>(b);
@@ -496,7 +588,8 @@ struct PointSet {
   __device__ __forceinline__ int64_t operator[](int64_t i) const { return list ? (int64_t)list[i] : i; }
 };
 
-template <typename T, int NB, int CX>
+// TW: arithmetic of the reduction that reads the workspace (the point stride depends on it).
+template <typename T, int NB, int CX, typename TW>
 __global__ void __launch_bounds__(16 * CX, 1) inverse_kernel(const float2* __restrict__ coh, PointSet pts, int n,
                                                           unsigned char* __restrict__ ws, uint8_t* __restrict__ sing,
                                                           float cond_max) {
@@ -519,7 +612,7 @@ __global__ void __launch_bounds__(16 * CX, 1) inverse_kernel(const float2* __res
       const T cond = anorm * max_abs_row_sum<T, NB, CX>(a, n, tx, ty, gs);
       if (!(cond <= (T)cond_max)) flag = kRouteCond;
     }
-    T* out = PointPtr<T>(ws, pt, n).ainv;
+    T* out = PointPtr<TW, T>(ws, pt, n).ainv;
 #pragma unroll
     for (int ib = 0; ib < NB; ++ib) {
       const int r0 = ty + 16 * ib;
@@ -530,7 +623,7 @@ __global__ void __launch_bounds__(16 * CX, 1) inverse_kernel(const float2* __res
         const int c0 = tx + CX * jb;
         if (c0 >= n) continue;
         const int pc = gs.piv_of_step[c0];
-        if (kr >= pc) out[(int64_t)kr * (kr + 1) / 2 + pc] = a[ib][jb];
+        if (kr >= pc) out[tri_up(pc, kr, n)] = a[ib][jb];  // inv[kr][pc], kept once
       }
     }
     if (tid == 0) sing[pt] = flag;
@@ -539,7 +632,7 @@ __global__ void __launch_bounds__(16 * CX, 1) inverse_kernel(const float2* __res
 }
 
 // ----------------------------------------------------------------- kernel 2: reduction
-template <typename T>
+template <typename T, typename TA>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 2) reduce_kernel(const float2* __restrict__ coh, PointSet pts, int n,
                                                          unsigned char* __restrict__ ws) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -550,21 +643,22 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 2) reduce_kerne
   const int64_t npt = pts.size();
   for (int64_t pt = blockIdx.x; pt < npt; pt += gridDim.x) {
     const float2* c = coh + pts[pt] * npairs;
-    PointPtr<T> w(ws, pt, n);
-    // M = inv(|Gamma|) o Gamma, lower triangle packed like inv(|Gamma|) itself
-    int i = 0;
-    while (tri(i + 1) <= tid) ++i;
+    PointPtr<T, TA> w(ws, pt, n);
+    // M = inv(|Gamma|) o Gamma: read along the upper triangle (inverse and coherence both
+    // contiguous), written to the packed lower triangle as M_jm = conj(M_mj)
+    int m = 0;
+    while (tri_up(m + 1, m + 1, n) <= tid) ++m;
     for (int q = tid; q < np; q += nt) {
-      while (tri(i + 1) <= q) ++i;
-      const int j = q - tri(i);
+      while (tri_up(m + 1, m + 1, n) <= q) ++m;
+      const int j = m + (q - (int)tri_up(m, m, n));
+      const TA sc = w.ainv[q];
       T gx = 1, gy = 0;
-      if (i != j) {
-        const float2 g = c[triu_index(j, i, n)];
+      if (j != m) {
+        const float2 g = c[(int64_t)q - (m + 1)];  // pair (m, j): triu_index(m, j) = tri_up(m, j) - m - 1
         gx = g.x;
-        gy = -g.y;  // Gamma_ij = conj(Gamma_ji) for i > j
+        gy = -g.y;
       }
-      const T sc = w.ainv[q];
-      s.L[q] = mk<T>(sc * gx, sc * gy);
+      s.L[tri(j) + m] = mk<T>((T)(sc * gx), (T)(sc * gy));
     }
     __syncthreads();
     tridiag_packed<T>(s, n);
@@ -588,7 +682,7 @@ __host__ __device__ inline size_t tail_warp_bytes(int n) {
   return align16(6 * (size_t)n * sizeof(T)) + align16((size_t)n * sizeof(C)) + align16((size_t)n * sizeof(double2));
 }
 
-template <typename T>
+template <typename T, typename TA>
 __global__ void __launch_bounds__(32 * kTailWarps, 3) tail_kernel(const float2* __restrict__ coh, PointSet pts, int n,
                                                               int ref, const unsigned char* __restrict__ ws,
                                                               const uint8_t* __restrict__ sing,
@@ -611,7 +705,7 @@ __global__ void __launch_bounds__(32 * kTailWarps, 3) tail_kernel(const float2* 
   const int64_t npt = pts.size();
   for (int64_t pt = (int64_t)blockIdx.x * kTailWarps + wid; pt < npt; pt += (int64_t)gridDim.x * kTailWarps) {
     const int64_t gp = pts[pt];
-    const PointPtr<T> w(const_cast<unsigned char*>(ws), pt, n);
+    const PointPtr<T, TA> w(const_cast<unsigned char*>(ws), pt, n);
     // real tridiagonal: b = |e|, phases delta_{k+1} = delta_k e_k/|e_k| (warp prefix product)
     C carry = mk<T>(1, 0);
     for (int k0 = 0; k0 < n; k0 += 32) {
@@ -754,6 +848,379 @@ __global__ void __launch_bounds__(32 * kTailWarps, 3) tail_kernel(const float2* 
   }
 }
 
+
+// ----------------------------------------------------------------- kernel 3b: refined tail
+// For the refined mixed precision (FP64 inverse, FP32 reduction): the FP32 eigenvector is
+// improved by one step of a Newton (Jacobi-Davidson) correction in FP64,
+//   r = M v - lambda v (lambda = v^H M v, M = inv(|Gamma|) o Gamma from the FP64 inverse),
+//   (M - lambda I) dv = r solved approximately through the FP32 factors M ~ Q D R D^H Q^H,
+//   dv = Q D P (R - lambda I)^-1 P D^H Q^H r, P the projector orthogonal to R's eigenvector,
+// which divides the error by about eps32 ||M|| / gap. Then the refined pair is checked in
+// FP64: with residual r', gap g = lambda_2(R) - lambda and smallest component |v_i|, the
+// phase error of every date is at most |r'| / (g min|v_i|); points above `tol` are flagged
+// for an FP64 recomputation. One warp per point.
+constexpr int kRefineWarps = 4;
+
+__host__ __device__ inline size_t refine_warp_bytes(int n) {
+  return align16(6 * (size_t)n * sizeof(float)) + align16(6 * (size_t)n * sizeof(double)) +
+         3 * align16((size_t)n * sizeof(double2));
+}
+
+// Solve (R - lambda I) x = y in place for a complex y, R real symmetric tridiagonal (d, b):
+// the elimination of tridiag_solve with the right-hand side carried as two real columns.
+__device__ inline void tridiag_solve_c(const double* d, const double* b, int n, double lambda, double tiny,
+                                       double2* y, double* dd, double* du, double* dl) {
+  for (int i = 0; i < n; ++i) {
+    dd[i] = d[i] - lambda;
+    if (i < n - 1) { du[i] = b[i]; dl[i] = b[i]; }
+  }
+  for (int i = 0; i < n - 1; ++i) {
+    const double sub = dl[i];
+    if (fabs(dd[i]) >= fabs(sub)) {
+      if (dd[i] == 0.0) dd[i] = tiny;
+      const double f = sub / dd[i];
+      dd[i + 1] -= f * du[i];
+      y[i + 1].x -= f * y[i].x;
+      y[i + 1].y -= f * y[i].y;
+      dl[i] = 0.0;
+    } else {
+      const double f = dd[i] / sub;
+      dd[i] = sub;
+      const double t = dd[i + 1];
+      dd[i + 1] = du[i] - f * t;
+      if (i < n - 2) {
+        dl[i] = du[i + 1];
+        du[i + 1] = -f * dl[i];
+      } else {
+        dl[i] = 0.0;
+      }
+      du[i] = t;
+      const double2 ty = y[i];
+      y[i] = y[i + 1];
+      y[i + 1] = make_double2(ty.x - f * y[i + 1].x, ty.y - f * y[i + 1].y);
+    }
+  }
+  if (dd[n - 1] == 0.0) dd[n - 1] = tiny;
+  y[n - 1].x /= dd[n - 1];
+  y[n - 1].y /= dd[n - 1];
+  if (n > 1) {
+    y[n - 2].x = (y[n - 2].x - du[n - 2] * y[n - 1].x) / dd[n - 2];
+    y[n - 2].y = (y[n - 2].y - du[n - 2] * y[n - 1].y) / dd[n - 2];
+  }
+  for (int i = n - 3; i >= 0; --i) {
+    y[i].x = (y[i].x - du[i] * y[i + 1].x - dl[i] * y[i + 2].x) / dd[i];
+    y[i].y = (y[i].y - du[i] * y[i + 1].y - dl[i] * y[i + 2].y) / dd[i];
+  }
+}
+
+// out = M v for M = inv(|Gamma|) o Gamma (Hermitian), read along the upper triangle: the
+// element (m, j > m) adds M_mj v_j to row m and conj(M_mj) v_m to row j. Lanes own columns
+// j = lane + 32 c; rows go four at a time through warp_sum4. One warp.
+__device__ void herm_matvec(const double* __restrict__ ainv, const float2* __restrict__ c, int n,
+                            const double2* v, double2* out) {
+  constexpr int NC = (kMaxFastN + 31) / 32;
+  const int lane = threadIdx.x & 31;
+  double2 vj[NC], cacc[NC];
+#pragma unroll
+  for (int t = 0; t < NC; ++t) {
+    const int j = lane + 32 * t;
+    vj[t] = j < n ? v[j] : make_double2(0, 0);
+    cacc[t] = make_double2(0, 0);
+  }
+  for (int m0 = 0; m0 < n; m0 += 4) {
+    double2 racc[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      racc[r] = make_double2(0, 0);
+      const int m = m0 + r;
+      if (m >= n) continue;  // warp-uniform
+      const double2 vm = v[m];
+      const int64_t um = tri_up(m, m, n), qm = um - (m + 1);
+#pragma unroll
+      for (int t = 0; t < NC; ++t) {
+        const int j = lane + 32 * t;
+        if (j < m || j >= n) continue;
+        const double s = ainv[um + (j - m)];
+        if (j == m) {
+          racc[r].x += s * vm.x;
+          racc[r].y += s * vm.y;
+        } else {
+          const float2 g = c[qm + (j - m)];
+          const double2 a = make_double2(s * (double)g.x, s * (double)g.y);  // M_mj
+          cmac(racc[r], a, vj[t]);
+          cmacc(cacc[t], a, vm);
+        }
+      }
+    }
+    const double2 tot = warp_sum4(racc);
+    const int r = lane >> 3;
+    if ((lane & 7) == 0 && m0 + r < n) out[m0 + r] = tot;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int t = 0; t < NC; ++t) {
+    const int j = lane + 32 * t;
+    if (j < n) out[j] = cadd(out[j], cacc[t]);
+  }
+  __syncwarp();
+}
+
+// z <- H_k z for the reflectors of the workspace, k ascending (forward, Q^H z) or
+// descending (back, Q z); the reflectors' FP32 values are used exactly, in FP64. One warp.
+template <typename T, typename TA>
+__device__ void apply_q(const PointPtr<T, TA>& w, int n, double2* z, bool forward) {
+  using C = typename C2<T>::type;
+  const int lane = threadIdx.x & 31;
+  for (int s = 0; s + 2 < n; ++s) {
+    const int k = forward ? s : n - 3 - s;
+    const double tau = (double)w.tau[k];
+    if (tau == 0.0) continue;
+    const C* u = w.refl + refl_off(k, n);
+    const int m = n - k - 1;
+    double2 acc = make_double2(0, 0), uu[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int i = lane + 32 * t;
+      uu[t] = make_double2(0, 0);
+      if (i < m) {
+        const C ui = u[i];
+        uu[t] = make_double2(ui.x, ui.y);
+        cmacc(acc, uu[t], z[k + 1 + i]);  // u^H z
+      }
+    }
+    acc.x = warp_sum(acc.x);
+    acc.y = warp_sum(acc.y);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int i = lane + 32 * t;
+      if (i < m) {
+        const double2 tt = cmul(uu[t], acc);
+        z[k + 1 + i].x -= tau * tt.x;
+        z[k + 1 + i].y -= tau * tt.y;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Smallest sigma (to the bisection's resolution) with at least `target` eigenvalues of the
+// real tridiagonal (d, b2) at or below it, by multisection over the warp from [lo, hi].
+template <typename T>
+__device__ T multisect(const T* d, const T* b2, int n, T lo, T hi, int target, T pivmin, int rounds) {
+  const int lane = threadIdx.x & 31;
+  const T eps = Lim<T>::eps();
+  for (int it = 0; it < rounds; ++it) {
+    const T width = hi - lo;
+    if (!(width > T(2) * eps * fmax(fabs(lo), fabs(hi)) + T(4) * pivmin)) break;
+    const T sg = lo + width * (T)(lane + 1) / T(33);
+    const int cnt = sturm_count(d, b2, n, sg, pivmin);
+    const unsigned ball = __ballot_sync(0xffffffffu, cnt >= target);
+    const int first = ball ? __ffs(ball) - 1 : 32;
+    const T nlo = (first == 0) ? lo : lo + width * (T)first / T(33);
+    const T nhi = (first == 32) ? hi : lo + width * (T)(first + 1) / T(33);
+    lo = nlo;
+    hi = nhi;
+  }
+  return T(0.5) * (lo + hi);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kRefineWarps) tail_refine_kernel(
+    const float2* __restrict__ coh, PointSet pts, int n, int ref, const unsigned char* __restrict__ ws,
+    uint8_t* __restrict__ sing, float2* __restrict__ ph, float* __restrict__ quality, float* __restrict__ tcoh,
+    double tol) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned char* mine = smem_raw + (size_t)wid * refine_warp_bytes(n);
+  T* d = reinterpret_cast<T*>(mine);
+  T* b = d + n;
+  T* b2 = b + n;
+  T* y = b2 + n;
+  T* w1 = y + n;
+  T* w2 = w1 + n;
+  double* dd = reinterpret_cast<double*>(mine + align16(6 * (size_t)n * sizeof(float)));
+  double* bd = dd + n;
+  double* yd = bd + n;
+  double* s1 = yd + n;
+  double* s2 = s1 + n;
+  double* s3 = s2 + n;
+  double2* dph = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(dd) + align16(6 * (size_t)n * sizeof(double)));
+  double2* v = dph + n;
+  double2* t1 = v + n;
+  const int64_t npairs = (int64_t)n * (n - 1) / 2;
+  const float fnan = __int_as_float(0x7fffffff);
+  const int64_t npt = pts.size();
+  for (int64_t pt = (int64_t)blockIdx.x * kRefineWarps + wid; pt < npt; pt += (int64_t)gridDim.x * kRefineWarps) {
+    const int64_t gp = pts[pt];
+    const PointPtr<T, double> w(const_cast<unsigned char*>(ws), pt, n);
+    const float2* c = coh + gp * npairs;
+    // real tridiagonal R: b = |e|, phases delta_{k+1} = delta_k e_k/|e_k| (warp prefix product, FP64)
+    double2 carry = make_double2(1, 0);
+    for (int k0 = 0; k0 < n; k0 += 32) {
+      const int k = k0 + lane;
+      if (k < n) { d[k] = w.d[k]; dd[k] = (double)w.d[k]; }
+      double2 f = make_double2(1, 0);
+      if (k + 1 < n) {
+        const typename C2<T>::type ek = w.e[k];
+        const double ex = ek.x, ey = ek.y, a = sqrt(ex * ex + ey * ey);
+        b[k] = (T)a;
+        b2[k] = (T)a * (T)a;
+        bd[k] = a;
+        if (a > 0.0) f = make_double2(ex / a, ey / a);
+      }
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double ox = __shfl_up_sync(0xffffffffu, f.x, o), oy = __shfl_up_sync(0xffffffffu, f.y, o);
+        if (lane >= o) f = cmul(make_double2(ox, oy), f);
+      }
+      const double2 dl = cmul(carry, f);
+      if (k0 == 0 && lane == 0) dph[0] = make_double2(1, 0);
+      if (k + 1 < n) dph[k + 1] = dl;
+      carry = make_double2(__shfl_sync(0xffffffffu, dl.x, 31), __shfl_sync(0xffffffffu, dl.y, 31));
+    }
+    __syncwarp();
+    // lambda_1 and lambda_2 of R (FP32 Sturm counts)
+    T lo = Lim<T>::huge(), hi = -Lim<T>::huge(), tnorm = 0;
+    for (int i = lane; i < n; i += 32) {
+      const T r = (i > 0 ? b[i - 1] : T(0)) + (i + 1 < n ? b[i] : T(0));
+      lo = fmin(lo, d[i] - r);
+      hi = fmax(hi, d[i] + r);
+      tnorm = fmax(tnorm, fabs(d[i]) + r);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+      tnorm = fmax(tnorm, __shfl_xor_sync(0xffffffffu, tnorm, o));
+    }
+    const T eps = Lim<T>::eps();
+    const T pivmin = fmax(Lim<T>::tiny(), eps * eps * tnorm * tnorm) + Lim<T>::tiny();
+    const T pad = T(2) * eps * fmax(tnorm, Lim<T>::tiny()) + T(2) * pivmin;
+    lo -= pad;
+    hi += pad;
+    const T lam1 = multisect(d, b2, n, lo, hi, 1, pivmin, 64);
+    const T lam2 = n > 1 ? multisect(d, b2, n, lo, hi, 2, pivmin, 6) : hi;
+    // eigenvector y of R by inverse iteration (FP32, lane 0)
+    for (int i = lane; i < n; i += 32) y[i] = T(1) + T(0.25) * (T)((i * 37) % 11) / T(11);
+    __syncwarp();
+    if (lane == 0) {
+      const T tiny = eps * fmax(tnorm, Lim<T>::tiny());
+      for (int it = 0; it < 2; ++it) {
+        tridiag_solve(d, b, n, lam1, tiny, y, w1, w2, b2);  // b2 is free after the bisections
+        T sc = 0;
+        for (int i = 0; i < n; ++i) sc = fmax(sc, fabs(y[i]));
+        if (!(sc > T(0)) || !isfinite(sc)) break;
+        const T r = T(1) / sc;
+        for (int i = 0; i < n; ++i) y[i] *= r;
+      }
+    }
+    __syncwarp();
+    // y to unit length in FP64; v = Q D y
+    double yn = 0;
+    for (int i = lane; i < n; i += 32) { yd[i] = (double)y[i]; yn += yd[i] * yd[i]; }
+    yn = 1.0 / sqrt(warp_sum(yn));
+    for (int i = lane; i < n; i += 32) {
+      yd[i] *= yn;
+      v[i] = make_double2(dph[i].x * yd[i], dph[i].y * yd[i]);
+    }
+    __syncwarp();
+    apply_q(w, n, v, false);
+    // one correction step, then the check
+    double lam = 0, rn = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+      herm_matvec(w.ainv, c, n, v, t1);
+      double vmv = 0, vv = 0;
+      for (int i = lane; i < n; i += 32) {
+        vmv += v[i].x * t1[i].x + v[i].y * t1[i].y;
+        vv += v[i].x * v[i].x + v[i].y * v[i].y;
+      }
+      vv = warp_sum(vv);
+      lam = warp_sum(vmv) / vv;
+      double r2 = 0;
+      for (int i = lane; i < n; i += 32) {
+        t1[i] = make_double2(t1[i].x - lam * v[i].x, t1[i].y - lam * v[i].y);
+        r2 += t1[i].x * t1[i].x + t1[i].y * t1[i].y;
+      }
+      rn = sqrt(warp_sum(r2) / vv);
+      __syncwarp();
+      if (pass == 1) break;
+      // dv = Q D P (R - lam I)^-1 P D^H Q^H r
+      apply_q(w, n, t1, true);
+      double2 pr = make_double2(0, 0);
+      for (int i = lane; i < n; i += 32) {
+        t1[i] = cmulc(t1[i], dph[i]);  // D^H: times conj(delta_i)
+        pr.x += yd[i] * t1[i].x;
+        pr.y += yd[i] * t1[i].y;
+      }
+      pr.x = warp_sum(pr.x);
+      pr.y = warp_sum(pr.y);
+      for (int i = lane; i < n; i += 32) { t1[i].x -= yd[i] * pr.x; t1[i].y -= yd[i] * pr.y; }
+      __syncwarp();
+      if (lane == 0) tridiag_solve_c(dd, bd, n, lam, DBL_EPSILON * (double)tnorm + DBL_MIN, t1, s1, s2, s3);
+      __syncwarp();
+      pr = make_double2(0, 0);
+      for (int i = lane; i < n; i += 32) { pr.x += yd[i] * t1[i].x; pr.y += yd[i] * t1[i].y; }
+      pr.x = warp_sum(pr.x);
+      pr.y = warp_sum(pr.y);
+      for (int i = lane; i < n; i += 32)
+        t1[i] = cmul(make_double2(t1[i].x - yd[i] * pr.x, t1[i].y - yd[i] * pr.y), dph[i]);
+      __syncwarp();
+      apply_q(w, n, t1, false);
+      double vn = 0;
+      for (int i = lane; i < n; i += 32) {
+        v[i] = make_double2(v[i].x - t1[i].x, v[i].y - t1[i].y);
+        vn += v[i].x * v[i].x + v[i].y * v[i].y;
+      }
+      vn = 1.0 / sqrt(warp_sum(vn));
+      for (int i = lane; i < n; i += 32) v[i] = make_double2(v[i].x * vn, v[i].y * vn);
+      __syncwarp();
+    }
+    // phase error bound of the refined vector (v has unit length)
+    double vmin = 1e300;
+    for (int i = lane; i < n; i += 32) vmin = fmin(vmin, sqrt(v[i].x * v[i].x + v[i].y * v[i].y));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vmin = fmin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+    const double gap = (double)lam2 - lam - 4.0 * (double)eps * (double)n * (double)tnorm;
+    const double bound = rn / (gap * vmin);
+    const bool singular = (sing[pt] & kRouteSingular) != 0;
+    const bool ok = singular || (gap > 0.0 && bound <= tol);
+    // normalise to the reference image
+    const double2 zr = v[ref];
+    for (int i = lane; i < n; i += 32) {
+      const double2 q = cmulc(v[i], zr);
+      const double a = sqrt(q.x * q.x + q.y * q.y);
+      float2 o = make_float2((float)(q.x / a), (float)(q.y / a));
+      if (singular) o = make_float2(fnan, fnan);
+      ph[gp * n + i] = o;
+      t1[i] = make_double2(o.x, o.y);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      quality[gp] = singular ? fnan : (float)lam;
+      sing[pt] = singular ? kRouteSingular : (ok ? 0 : kRouteCond);
+    }
+    if (tcoh) {  // |sum_q coh_q/|coh_q| conj(ph_m) ph_j| / n_pairs
+      double tx = 0, ty = 0;
+      int mm = 0, jj = 1 + lane;
+      while (jj >= n && mm < n - 1) { mm += 1; jj = jj - n + mm + 1; }
+      for (int64_t q = lane; q < npairs; q += 32) {
+        const int m0 = mm, j0 = jj;
+        jj += 32;
+        while (jj >= n && mm < n - 1) { mm += 1; jj = jj - n + mm + 1; }
+        const float2 g = c[q];
+        const double ga = sqrt((double)g.x * g.x + (double)g.y * g.y);
+        const double2 q2 = cmul(make_double2(g.x / ga, g.y / ga), cmulc(t1[j0], t1[m0]));
+        tx += q2.x;
+        ty += q2.y;
+      }
+      tx = warp_sum(tx);
+      ty = warp_sum(ty);
+      if (lane == 0) tcoh[gp] = (float)(sqrt(tx * tx + ty * ty) / (double)npairs);
+    }
+    __syncwarp();
+  }
+}
+
 // ----------------------------------------------------------------- host side
 template <class K>
 int occupancy(K kernel, int threads, size_t smem) {
@@ -764,7 +1231,7 @@ int occupancy(K kernel, int threads, size_t smem) {
 
 template <typename T>
 int64_t sub_batch(int n) {
-  const PointWs<T> w(n);
+  const PointWs<T> w(n);  // FP64 sub-batches also fit the refined layout (it is smaller)
   return (int64_t)std::max<size_t>(1024, std::min<size_t>(1 << 17, (size_t)(1ull << 30) / (w.bytes + 1)));
 }
 
@@ -793,62 +1260,92 @@ struct SubWs {
   }
 };
 
+// List of the points to redo in FP64. `refined`: points singular in the (already FP64)
+// inverse are not redone.
 __global__ void route_kernel(const uint8_t* __restrict__ sing, int64_t nb, int32_t* __restrict__ list,
-                             int32_t* __restrict__ count, uint8_t* __restrict__ route) {
+                             int32_t* __restrict__ count, uint8_t* __restrict__ route, bool refined) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (int64_t)gridDim.x * blockDim.x) {
     const uint8_t f = sing[i];
     if (route) route[i] = f;
-    if (f) list[atomicAdd(count, 1)] = (int32_t)i;  // list order is free: points are independent
+    if (f && !(refined && f == kRouteSingular)) list[atomicAdd(count, 1)] = (int32_t)i;  // order is free
   }
 }
 
-// Column groups of the Gauss-Jordan grid. 32 groups (512 threads, half the registers per
-// thread) measured no faster than 16 in FP32 or FP64: one point per SM either way, and its
-// serial pivot steps set the pace.
+// Column groups of the Gauss-Jordan grid: 32 (512 threads), which halves the registers a
+// thread holds and leaves room for the look-ahead column.
 template <typename T>
-constexpr int gj_cx() { return 16; }
+constexpr int gj_cx() { return 32; }
 
-template <typename T, int NB>
+template <typename T, int NB, typename TW>
 int launch_inverse(const float2* coh, PointSet pts, int64_t grid_cap, int n, unsigned char* ws, uint8_t* sing,
                    float cond_max, cudaStream_t s) {
   constexpr int CX = gj_cx<T>();
-  const int occ = std::max(1, occupancy(inverse_kernel<T, NB, CX>, 16 * CX, 0));
+  const int occ = std::max(1, occupancy(inverse_kernel<T, NB, CX, TW>, 16 * CX, 0));
   const int64_t grid = std::min<int64_t>(grid_cap, (int64_t)sm_count() * occ);
-  inverse_kernel<T, NB, CX><<<(unsigned)grid, 16 * CX, 0, s>>>(coh, pts, n, ws, sing, cond_max);
+  inverse_kernel<T, NB, CX, TW><<<(unsigned)grid, 16 * CX, 0, s>>>(coh, pts, n, ws, sing, cond_max);
   return check_launch("emi inverse");
 }
 
+// inv(|Gamma|) in arithmetic TA into a workspace laid out for a reduction in T.
+template <typename TA, typename T>
+int run_inverse(const float2* c, PointSet pts, int n, unsigned char* ws, uint8_t* sing, float cond_max,
+                cudaStream_t s) {
+  const int64_t cap = pts.n_pc;  // grid bound: the most points this pass can see
+  switch ((n + 15) / 16) {
+    case 1: case 2: return launch_inverse<TA, 2, T>(c, pts, cap, n, ws, sing, cond_max, s);
+    case 3: return launch_inverse<TA, 3, T>(c, pts, cap, n, ws, sing, cond_max, s);
+    case 4: return launch_inverse<TA, 4, T>(c, pts, cap, n, ws, sing, cond_max, s);
+    case 5: return launch_inverse<TA, 5, T>(c, pts, cap, n, ws, sing, cond_max, s);
+    case 6: return launch_inverse<TA, 6, T>(c, pts, cap, n, ws, sing, cond_max, s);
+    case 7: return launch_inverse<TA, 7, T>(c, pts, cap, n, ws, sing, cond_max, s);
+    default: return launch_inverse<TA, 8, T>(c, pts, cap, n, ws, sing, cond_max, s);
+  }
+}
+
+template <typename T, typename TA>
+int run_reduce(const float2* c, PointSet pts, int n, unsigned char* ws, cudaStream_t s) {
+  const size_t rsmem = tri_bytes<T>(n);
+  if (int rc_ = allow_smem(reinterpret_cast<const void*>(reduce_kernel<T, TA>), (size_t)(rsmem))) return rc_;
+  const int rocc = occupancy(reduce_kernel<T, TA>, kThreads, rsmem);
+  if (rocc < 1) return fail(MR_ERR_UNSUPPORTED, "emi: %zu bytes of shared memory per CTA do not fit", rsmem);
+  reduce_kernel<T, TA><<<(unsigned)std::min<int64_t>(pts.n_pc, (int64_t)sm_count() * rocc), kThreads, rsmem, s>>>(
+      c, pts, n, ws);
+  return check_launch("emi reduce");
+}
+
 // One pass of the three kernels over a sub-batch (pts.list == nullptr: all pts.n_pc points;
-// else the listed ones, whose count is read on the device). cond_max > 0 flags the points
-// whose condition estimate exceeds it.
+// else the listed ones, whose count is read on the device), inverse and reduction both in
+// T. cond_max > 0 flags the points whose condition estimate exceeds it.
 template <typename T>
 int run_pass(const float2* c, PointSet pts, int n, int ref, float2* ph, float* quality, float* tcoh,
              unsigned char* ws, uint8_t* sing, float cond_max, cudaStream_t s) {
-  const int64_t cap = pts.n_pc;  // grid bound: the most points this pass can see
-  int rc;
-  switch ((n + 15) / 16) {
-    case 1: case 2: rc = launch_inverse<T, 2>(c, pts, cap, n, ws, sing, cond_max, s); break;
-    case 3: rc = launch_inverse<T, 3>(c, pts, cap, n, ws, sing, cond_max, s); break;
-    case 4: rc = launch_inverse<T, 4>(c, pts, cap, n, ws, sing, cond_max, s); break;
-    case 5: rc = launch_inverse<T, 5>(c, pts, cap, n, ws, sing, cond_max, s); break;
-    case 6: rc = launch_inverse<T, 6>(c, pts, cap, n, ws, sing, cond_max, s); break;
-    case 7: rc = launch_inverse<T, 7>(c, pts, cap, n, ws, sing, cond_max, s); break;
-    default: rc = launch_inverse<T, 8>(c, pts, cap, n, ws, sing, cond_max, s); break;
-  }
-  if (rc) return rc;
-  const size_t rsmem = tri_bytes<T>(n);
-  if (int rc_ = allow_smem(reinterpret_cast<const void*>(reduce_kernel<T>), (size_t)(rsmem))) return rc_;
-  const int rocc = occupancy(reduce_kernel<T>, kThreads, rsmem);
-  if (rocc < 1) return fail(MR_ERR_UNSUPPORTED, "emi: %zu bytes of shared memory per CTA do not fit", rsmem);
-  reduce_kernel<T><<<(unsigned)std::min<int64_t>(cap, (int64_t)sm_count() * rocc), kThreads, rsmem, s>>>(c, pts, n,
-                                                                                                        ws);
-  if (int e = check_launch("emi reduce")) return e;
+  if (int rc = run_inverse<T, T>(c, pts, n, ws, sing, cond_max, s)) return rc;
+  if (int rc = run_reduce<T, T>(c, pts, n, ws, s)) return rc;
   const size_t tsmem = kTailWarps * tail_warp_bytes<T>(n);
-  if (int rc_ = allow_smem(reinterpret_cast<const void*>(tail_kernel<T>), (size_t)(tsmem))) return rc_;
-  const int tocc = std::max(1, occupancy(tail_kernel<T>, 32 * kTailWarps, tsmem));
-  const int64_t tgrid = std::min<int64_t>((cap + kTailWarps - 1) / kTailWarps, (int64_t)sm_count() * tocc);
-  tail_kernel<T><<<(unsigned)tgrid, 32 * kTailWarps, tsmem, s>>>(c, pts, n, ref, ws, sing, ph, quality, tcoh);
+  if (int rc_ = allow_smem(reinterpret_cast<const void*>(tail_kernel<T, T>), (size_t)(tsmem))) return rc_;
+  const int tocc = std::max(1, occupancy(tail_kernel<T, T>, 32 * kTailWarps, tsmem));
+  const int64_t tgrid = std::min<int64_t>((pts.n_pc + kTailWarps - 1) / kTailWarps, (int64_t)sm_count() * tocc);
+  tail_kernel<T, T><<<(unsigned)tgrid, 32 * kTailWarps, tsmem, s>>>(c, pts, n, ref, ws, sing, ph, quality, tcoh);
   return check_launch("emi tail");
+}
+
+// The refined pass: FP64 inverse, FP32 reduction, FP64-refined tail; sing[] ends with the
+// points whose refined error bound exceeds `tol` flagged kRouteCond.
+int run_refine_pass(const float2* c, PointSet pts, int n, int ref, float2* ph, float* quality, float* tcoh,
+                    unsigned char* ws, uint8_t* sing, double tol, cudaStream_t s) {
+  if (int rc = run_inverse<double, float>(c, pts, n, ws, sing, 0.f, s)) return rc;
+  if (int rc = run_reduce<float, double>(c, pts, n, ws, s)) return rc;
+  const size_t tsmem = kRefineWarps * refine_warp_bytes(n);
+  if (int rc_ = allow_smem(reinterpret_cast<const void*>(tail_refine_kernel<float>), tsmem)) return rc_;
+  const int tocc = std::max(1, occupancy(tail_refine_kernel<float>, 32 * kRefineWarps, tsmem));
+  const int64_t tgrid = std::min<int64_t>((pts.n_pc + kRefineWarps - 1) / kRefineWarps, (int64_t)sm_count() * tocc);
+  tail_refine_kernel<float><<<(unsigned)tgrid, 32 * kRefineWarps, tsmem, s>>>(c, pts, n, ref, ws, sing, ph,
+                                                                                quality, tcoh, tol);
+  return check_launch("emi refine tail");
+}
+
+size_t point_bytes_max(int n) {
+  return std::max({PointWs<float>(n).bytes, PointWs<double>(n).bytes, PointWs<float, double>(n).bytes});
 }
 
 }  // namespace
@@ -858,20 +1355,22 @@ int fast_supported(int n) { return n >= 2 && n <= kMaxFastN; }
 size_t fast_workspace_bytes(int64_t n_pc, int n) {
   const int64_t s32 = std::min<int64_t>(n_pc, sub_batch<float>(n));
   const int64_t s64 = std::min<int64_t>(n_pc, sub_batch<double>(n));
-  return std::max(SubWs::bytes(s32, PointWs<float>(n).bytes), SubWs::bytes(s64, PointWs<double>(n).bytes));
+  return std::max(SubWs::bytes(s32, PointWs<float>(n).bytes), SubWs::bytes(s64, point_bytes_max(n)));
 }
 
 int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, float cond_max, float2* ph,
              float* quality, float* tcoh, uint8_t* route, void* workspace, cudaStream_t s,
              const int64_t* dcount, int64_t doff) {
-  if (dcount && precision == MR_PREC_MIXED)
-    return fail(MR_ERR_UNSUPPORTED, "emi: device-counted points run in FP32 or FP64");
-  auto* ws = static_cast<unsigned char*>(workspace);
   const bool f64 = precision == MR_PREC_FP64;
   const bool mixed = precision == MR_PREC_MIXED;
-  // a mixed sub-batch must hold its points in FP64 when all of them are routed
-  const int64_t sub = std::min<int64_t>(n_pc, (f64 || mixed) ? sub_batch<double>(n) : sub_batch<float>(n));
-  const SubWs w(ws, sub, f64 || mixed ? PointWs<double>(n).bytes : PointWs<float>(n).bytes);
+  const bool refine = precision == MR_PREC_REFINE;
+  if (dcount && (mixed || refine))
+    return fail(MR_ERR_UNSUPPORTED, "emi: device-counted points run in FP32 or FP64");
+  auto* ws = static_cast<unsigned char*>(workspace);
+  // a mixed or refined sub-batch must hold its points in FP64 when all of them are routed
+  const bool wide = f64 || mixed || refine;
+  const int64_t sub = std::min<int64_t>(n_pc, wide ? sub_batch<double>(n) : sub_batch<float>(n));
+  const SubWs w(ws, sub, wide ? point_bytes_max(n) : PointWs<float>(n).bytes);
   const int64_t npairs = (int64_t)n * (n - 1) / 2;
   for (int64_t b0 = 0; b0 < n_pc; b0 += sub) {
     const int64_t nb = std::min<int64_t>(sub, n_pc - b0);
@@ -885,11 +1384,12 @@ int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, flo
       rc = run_pass<double>(c, all, n, ref, p, q, t, w.pts, w.sing, 0.f, s);
       if (!rc && route) MR_CUDA_TRY(cudaMemsetAsync(route + b0, 1, (size_t)nb, s));
     } else {
-      rc = run_pass<float>(c, all, n, ref, p, q, t, w.pts, w.sing, mixed ? cond_max : 0.f, s);
-      if (!rc && mixed) {
+      rc = refine ? run_refine_pass(c, all, n, ref, p, q, t, w.pts, w.sing, (double)cond_max, s)
+                  : run_pass<float>(c, all, n, ref, p, q, t, w.pts, w.sing, mixed ? cond_max : 0.f, s);
+      if (!rc && (mixed || refine)) {
         MR_CUDA_TRY(cudaMemsetAsync(w.count, 0, sizeof(int32_t), s));
         const int grid = (int)std::min<int64_t>((nb + 255) / 256, (int64_t)sm_count() * 8);
-        route_kernel<<<grid, 256, 0, s>>>(w.sing, nb, w.list, w.count, route ? route + b0 : nullptr);
+        route_kernel<<<grid, 256, 0, s>>>(w.sing, nb, w.list, w.count, route ? route + b0 : nullptr, refine);
         rc = check_launch("emi route");
         if (!rc) rc = run_pass<double>(c, PointSet{w.list, w.count, nb}, n, ref, p, q, t, w.pts, w.sing2, 0.f, s);
       } else if (!rc && route) {

@@ -161,26 +161,60 @@ extern "C" int mr_ds_extract(const int32_t* shp_num, const uint8_t* is_shp, int 
 // (kNoAllocMaxBlocks * 8 bytes = 128 KiB per device). Its address is a device address,
 // which host code must look up per device (cudaGetSymbolAddress) before passing it to a
 // kernel: the symbol's name in host code is only a host-side stand-in.
+#include <cuda.h>
+
 #include <mutex>
 
 namespace mr {
 namespace {
 
 constexpr int64_t kNoAllocMaxBlocks = 16384;  // rasters up to 16384 * 1024 = 16,777,216 pixels
+static_assert(kNoAllocMaxBlocks * kBlk == MR_DS_EXTRACT_NOALLOC_MAX_PIXELS,
+              "the header's pixel limit must match the compiled array");
 static __device__ __align__(256) int64_t g_extract_counts[kNoAllocMaxBlocks];
 
-// Device address of g_extract_counts on the current device, looked up once per device.
+// ID of the calling thread's current CUDA context (0 if none or if the driver cannot tell).
+// The driver's functions come through the runtime, so the library needs no libcuda link.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault) == cudaSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault) == cudaSuccess) get_id = reinterpret_cast<GetId>(f);
+    cudaGetLastError();
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of g_extract_counts in the current context. The module that holds the
+// array is loaded once per context, so the address is looked up (cudaGetSymbolAddress,
+// with the device current) on the first call in a context and kept with that context's
+// ID: a context torn down and created again (cudaDeviceReset) gets a new ID, and the
+// next call looks the address up again instead of using a stale one.
 int noalloc_counts(int64_t** out) {
   static std::mutex mu;
+  static unsigned long long ctx_of[64] = {0};
   static int64_t* addr[64] = {nullptr};
   int dev = 0;
   MR_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(MR_ERR_UNSUPPORTED, "ds_extract_noalloc: device index %d", dev);
   std::lock_guard<std::mutex> lock(mu);
-  if (addr[dev] == nullptr) {
+  const unsigned long long id = current_context_id();
+  if (addr[dev] == nullptr || id == 0 || id != ctx_of[dev]) {
     void* p = nullptr;
     MR_CUDA_TRY(cudaGetSymbolAddress(&p, g_extract_counts));
     addr[dev] = static_cast<int64_t*>(p);
+    ctx_of[dev] = current_context_id();  // the lookup made the primary context current if none was
   }
   *out = addr[dev];
   return MR_OK;

@@ -14,10 +14,12 @@ __all__ = ["emi", "ds_temp_coh", "emperical_co_emi_temp_coh_pc"]
 
 
 EMI_COND_MAX = 1.0e4
+EMI_REFINE_TOL = 1.0e-4
 
 
 def _emi_device(c: torch.Tensor, nimages: int, ref: int, want_tcoh: bool = False, precision: str = "fp64",
-                cond_max: float = EMI_COND_MAX, route: torch.Tensor | None = None):
+                cond_max: float = EMI_COND_MAX, route: torch.Tensor | None = None,
+                refine_tol: float = EMI_REFINE_TOL):
     dev = c.device
     n_pc = c.shape[0]
     ph = torch.empty((n_pc, nimages), dtype=torch.complex64, device=dev)
@@ -28,34 +30,42 @@ def _emi_device(c: torch.Tensor, nimages: int, ref: int, want_tcoh: bool = False
     if precision == "mixed":
         _lib.call("mr_emi_routed", c.data_ptr(), n_pc, nimages, ref, float(cond_max), ph.data_ptr(), q.data_ptr(),
                   _dev.ptr(t), _dev.ptr(route), ws.data_ptr(), ws.numel(), _dev.stream())
+    elif precision == "refine":
+        _lib.call("mr_emi_refined", c.data_ptr(), n_pc, nimages, ref, float(refine_tol), ph.data_ptr(),
+                  q.data_ptr(), _dev.ptr(t), _dev.ptr(route), ws.data_ptr(), ws.numel(), _dev.stream())
     else:
         _lib.call("mr_emi", c.data_ptr(), n_pc, nimages, ref, _lib.PREC[precision], ph.data_ptr(), q.data_ptr(),
                   _dev.ptr(t), ws.data_ptr(), ws.numel(), _dev.stream())
     return ph, q, t
 
 
-def emi(coh, ref: int = 0, precision: str = "fp64", cond_max: float = EMI_COND_MAX, return_route: bool = False):
+def emi(coh, ref: int = 0, precision: str = "fp64", cond_max: float = EMI_COND_MAX, return_route: bool = False,
+        refine_tol: float = EMI_REFINE_TOL):
     """EMI phase linking of compressed coherence ``(n_pc, n_pairs)`` (all pairs).
 
     Returns ``ph`` (n_pc, N) complex64 (unit modulus, ``ph[:, ref]`` real positive) and
     ``emi_quality`` (n_pc,) float32, the smallest eigenvalue of ``inv(|Gamma|) o Gamma``
     (moraine/pl.py:19-77). Additions to the reference signature: ``precision`` of the whole
-    computation, ``"fp64"`` (default), ``"fp32"`` or ``"mixed"`` (FP32, with the points
+    computation, ``"fp64"`` (default), ``"fp32"``, ``"mixed"`` (FP32, with the points
     whose cond_1(|Gamma|) estimate exceeds ``cond_max`` or that are singular in FP32
-    redone in FP64); ``return_route=True`` (mixed only) adds a uint8 array of the route of
-    every point (0 FP32, 1 FP64 by condition, 2 FP64 as singular in FP32).
+    redone in FP64) or ``"refine"`` (FP64 inverse of |Gamma|, FP32 reduction, one FP64
+    refinement step of the eigenvector, and the points whose phase error bound exceeds
+    ``refine_tol`` rad redone in FP64); ``return_route=True`` (mixed or refine) adds a
+    uint8 array of the route of every point (mixed: 0 FP32, 1 FP64 by condition, 2 FP64 as
+    singular in FP32; refine: 0 refined, 1 redone in FP64, 2 singular).
     """
-    if precision not in ("fp32", "fp64", "mixed"):
-        raise ValueError(f"emi: precision must be 'fp32', 'fp64' or 'mixed', not {precision!r}")
-    if return_route and precision != "mixed":
-        raise ValueError("emi: return_route needs precision='mixed'")
+    if precision not in ("fp32", "fp64", "mixed", "refine"):
+        raise ValueError(f"emi: precision must be 'fp32', 'fp64', 'mixed' or 'refine', not {precision!r}")
+    if return_route and precision not in ("mixed", "refine"):
+        raise ValueError("emi: return_route needs precision='mixed' or 'refine'")
     kind = _dev.kind_of(coh)
     dev = _dev.require_cuda()
     c = _dev.to_device(coh, torch.complex64, dev)
     nimages = nimage_from_npair(c.shape[-1])
     c2 = c.reshape(-1, c.shape[-1])
     route = torch.empty((c2.shape[0],), dtype=torch.uint8, device=dev) if return_route else None
-    ph, q, _ = _emi_device(c2, nimages, int(ref), precision=precision, cond_max=cond_max, route=route)
+    ph, q, _ = _emi_device(c2, nimages, int(ref), precision=precision, cond_max=cond_max, route=route,
+                           refine_tol=refine_tol)
     ph = ph.reshape(tuple(c.shape[:-1]) + (nimages,))
     q = q.reshape(tuple(c.shape[:-1]))
     if return_route:

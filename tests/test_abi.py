@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_version_and_sizes():
     lib = _lib.load()
-    assert lib.mr_abi_version() == 2
+    assert lib.mr_abi_version() == 3
     assert lib.mr_ks_workspace_bytes(200, 200, 17) == 200 * 200 * 20 * 4
     assert lib.mr_ks_workspace_bytes(0, 200, 17) == 0
     assert lib.mr_ds_extract_workspace_bytes(4096) == 4 * 8
@@ -60,7 +60,7 @@ C_HOST = r"""
 
 int main(void) {
   /* host-side paths only: no device memory, no kernel */
-  if (mr_abi_version() != 2) return 1;
+  if (mr_abi_version() != 3) return 1;
   if (mr_gamma_sample_bytes(MR_GAMMA_FCOMPLEX) != 8) return 2;
   if (mr_ks_workspace_bytes(100, 100, 17) == 0) return 3;
   if (mr_ds_chain_workspace_bytes(64, 64, 20, 2, 3, 1000) == 0) return 4;

@@ -40,3 +40,9 @@ def test_reference_arm_under_torchrun_prints_once():
     assert out.returncode == 0, out.stderr[-2000:]
     (d,) = _lines(out.stdout)
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+
+
+def test_ours_arm_rejects_zero_warmup():
+    out = subprocess.run([sys.executable, str(REPO / "bench.py"), "--warmup", "0", "--steps", "1"],
+                         capture_output=True, text=True, timeout=120, cwd=REPO)
+    assert out.returncode == 2 and "--warmup must be at least 1" in out.stderr

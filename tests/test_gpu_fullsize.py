@@ -1,9 +1,11 @@
 """Parity at full size: the 2000 x 2000 x 100 scene through the FP64 device chain.
 
-Too large for the oracle as a whole, so the whole-scene result is checked through
-properties that hold at any size (KS symmetry, the centre always an SHP, counts equal to
-the masks, DS indices in row-major order), and sampled DS points are checked against the
-oracle on the crop of their own window, which holds everything their result depends on.
+The SHP masks and counts of the whole scene are compared bit for bit with the oracle's KS
+selection (C, all host cores). The rest of the chain is too heavy for the oracle as a
+whole, so the whole-scene result is also checked through properties that hold at any size
+(KS symmetry, the centre always an SHP, counts equal to the masks, DS indices in row-major
+order), and sampled DS points are checked against the oracle on the crop of their own
+window, which holds everything their result depends on.
 """
 import numpy as np
 import pytest
@@ -28,6 +30,15 @@ def c2_full(cuda):
     res = chain.run(z)
     torch.cuda.synchronize()
     return cfg, z, res
+
+
+def test_fullsize_masks_bit_exact_vs_oracle(c2_full):
+    cfg, z, res = c2_full
+    rmli = O.intensity(z.cpu().numpy())
+    is_shp, num = O.ks_select(rmli, cfg.az_half_win, cfg.r_half_win, cfg.p_max)
+    np.testing.assert_array_equal(res.shp_num.cpu().numpy(), num)
+    dev = res.is_shp.cpu().numpy().view(bool)
+    assert np.array_equal(dev, is_shp), int(np.count_nonzero(dev != is_shp))
 
 
 def test_fullsize_mask_properties(c2_full):

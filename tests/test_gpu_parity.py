@@ -218,6 +218,57 @@ def test_emi_mixed_routing(cuda, name, size):
         mb.emi(coh.cpu().numpy(), precision="fp32", return_route=True)
 
 
+@pytest.mark.parametrize("name,size", [("c0", 64), ("c1", 40), ("c2", 40), ("c3", 24)])
+def test_emi_refine_vs_fp64_oracle(cuda, name, size):
+    """Refined mixed precision (FP64 inverse, FP32 reduction, one FP64 refinement step):
+    kept points are within their own bound (1e-4 rad) of the FP64 computation, points
+    redone in FP64 equal the FP64 run bit for bit, and the route follows the bound."""
+    cfg = CONFIGS[name].scaled(nlines=size, width=size)
+    z = make_stack(cfg).numpy()
+    p = O.ks_test(O.intensity(z), cfg.az_half_win, cfg.r_half_win)
+    is_shp, num = O.select_shp(p, cfg.p_max)
+    idx, pc = O.ds_candidates(is_shp, num, 1)
+    coh = O.emperical_co_pc(z, idx, pc).astype(np.complex64)
+    ph_r, q_r, gap, cond = O.emi(coh)
+    ph, q, route = mb.emi(coh, precision="refine", return_route=True)
+    ph64, q64 = mb.emi(coh, precision="fp64")
+    assert set(np.unique(route)) <= {0, 1, 2}
+    kept, redone = route == 0, route == 1
+    assert kept.mean() > 0.5
+    tol64 = O.phase_tolerance(cond, gap, eps=1e3 * EPS64, floor=3e-7)
+    err = np.abs(np.angle(ph * np.conj(ph_r))).max(-1)
+    assert np.all(err[kept] <= tol64[kept] + 1e-4), (err[kept] - tol64[kept]).max()
+    # the refinement reaches FP64-class accuracy on the typical point
+    assert np.median(err[kept]) < 1e-6
+    np.testing.assert_array_equal(ph[redone].view(np.int32), ph64[redone].view(np.int32))
+    np.testing.assert_array_equal(q[redone].view(np.int32), q64[redone].view(np.int32))
+    assert np.all(np.isnan(ph[route == 2]))
+    qtol = np.maximum(1e-5, 1e3 * EPS64 * cond) * np.maximum(1, np.abs(q_r))
+    assert np.all(np.abs(q - q_r)[kept] <= qtol[kept])
+    # a bound nothing meets sends every point to FP64; one everything meets keeps them all
+    _, _, r0 = mb.emi(coh, precision="refine", return_route=True, refine_tol=1e-30)
+    assert np.all(r0 != 0)
+    ph1, _, r1 = mb.emi(coh, precision="refine", return_route=True, refine_tol=1e30)
+    assert not np.any(r1 == 1)
+    np.testing.assert_array_equal(ph1[kept].view(np.int32), ph[kept].view(np.int32))
+
+
+def test_chain_refine_route(cuda):
+    cfg = CONFIGS["c2"].scaled(nlines=40, width=40)
+    z = make_stack(cfg, device=cuda)
+    kw = dict(device=cuda, precision="fp64")
+    res = DsChain(40, 40, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, 1, emi_precision="refine",
+                  **kw).run(z)
+    ref = DsChain(40, 40, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, 1, **kw).run(z)
+    assert res.route is not None and res.route.shape == (res.n_ds,)
+    err = (res.ph * ref.ph.conj()).angle().abs().amax(-1)
+    keep = res.route == 0
+    assert keep.float().mean() > 0.5
+    assert float(err[keep].max()) < 2e-4
+    again = (res.route == 1)
+    assert torch.equal(res.ph[again], ref.ph[again])
+
+
 def test_chain_mixed_route(cuda):
     cfg = CONFIGS["c3"].scaled(nlines=24, width=24, nimages=64)
     z = make_stack(cfg, device=cuda)
@@ -308,6 +359,34 @@ def test_device_chain_vs_reference_fixture(cuda, golden):
     assert np.all(err <= tol), (err / tol).max()
     well = tol < 1e-3
     assert np.abs(res.t_coh.cpu().numpy() - g["t_coh"])[well].max(initial=0) < 1e-3
+
+
+@pytest.mark.parametrize("name", ["chain_c1_n50", "chain_c2_n100"])
+@pytest.mark.parametrize("emi", ["fp64", "refine"])
+def test_device_chain_vs_reference_at_image_counts(cuda, golden, name, emi):
+    """The device chain against the reference's own chain at the benchmark image counts
+    (N = 50 and N = 100): masks and counts bit-exact, FP64 coherence, phases within the
+    reference's complex64 EMI bound, temporal coherence of the reference phases."""
+    g = golden(f"{name}.npz")
+    rslc = g["rslc"]
+    nl, w, n = rslc.shape
+    azh, rh = (int(v) for v in g["win"])
+    ch = DsChain(nl, w, n, azh, rh, p_max=float(g["p_max"]), min_shp=int(g["min_shp"]), precision="fp64",
+                 emi_precision=emi)
+    res = ch.run(torch.from_numpy(rslc).to(cuda))
+    np.testing.assert_array_equal(np.packbits(res.is_shp.cpu().numpy().astype(bool).reshape(-1)), g["is_shp_bits"])
+    np.testing.assert_array_equal(res.shp_num.cpu().numpy(), g["shp_num"])
+    k = g["idx"].shape[0]
+    np.testing.assert_array_equal(res.idx.cpu().numpy()[:k], g["idx"])
+    is_shp = np.unpackbits(g["is_shp_bits"]).astype(bool).reshape(nl, w, 2 * azh + 1, 2 * rh + 1)
+    pc = is_shp[tuple(g["idx"].T)]
+    coh = mb.emperical_co_pc(rslc, g["idx"], pc, precision="fp64")
+    np.testing.assert_allclose(coh[:8], g["coh_head"], atol=2e-7)
+    _, _, gap, cond = O.emi(coh)
+    tol = O.phase_tolerance(cond, gap, eps=4 * EPS32)
+    err = np.abs(np.angle(res.ph.cpu().numpy()[:k] * np.conj(g["ph"]))).max(-1)
+    assert np.all(err <= tol), (err / tol).max()
+    np.testing.assert_allclose(mb.ds_temp_coh(coh, g["ph"]), g["t_coh"], atol=5e-5)
 
 
 @pytest.mark.parametrize("name,size", [("c0", 200), ("c1", 96), ("c2", 96)])

@@ -5,7 +5,8 @@ memory; it keeps its scratch in a fixed array compiled into the library. This fi
 named to be collected last, so a run that stops at its first failure has already run
 every other test.
 """
-import ctypes
+import re
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -14,6 +15,15 @@ import torch
 from moraine_b200 import _dev, _lib
 
 pytestmark = pytest.mark.gpu
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "moraine_b200.h"
+
+
+def _limit() -> int:
+    """MR_DS_EXTRACT_NOALLOC_MAX_PIXELS as the header defines it."""
+    m = re.search(r"#define MR_DS_EXTRACT_NOALLOC_MAX_PIXELS \((\d+)LL \* (\d+)LL\)", HEADER.read_text())
+    assert m, "limit macro not found in the header"
+    return int(m.group(1)) * int(m.group(2))
 
 
 def _raster(shape, win, seed, device):
@@ -56,10 +66,24 @@ def test_noalloc_matches_workspace_variant_twice(cuda):
         np.testing.assert_array_equal(pc, pc_ref)
 
 
+def test_noalloc_at_the_limit(cuda):
+    # a raster of exactly the limit fills the whole array and is accepted
+    limit = _limit()
+    nl = 4096
+    w = limit // nl
+    assert nl * w == limit
+    shp_num, is_shp = _raster((nl, w), 5, 3, cuda)
+    k_ref, idx_ref, pc_ref = _extract(False, shp_num, is_shp, 2)
+    k, idx, pc = _extract(True, shp_num, is_shp, 2)
+    assert k == k_ref and k > 0
+    np.testing.assert_array_equal(idx, idx_ref)
+    np.testing.assert_array_equal(pc, pc_ref)
+
+
 def test_noalloc_rejects_oversize_raster(cuda):
     lib = _lib.load()
-    limit = 16384 * 1024
-    nl, w = 4097, 4096  # one row more than the limit
+    limit = _limit()
+    nl, w = 4097, limit // 4096  # one row more than the limit
     assert nl * w > limit
     rc = lib.mr_ds_extract_noalloc(16, None, nl, w, 9, 3, 16, None, 100, 16, None)
     assert rc == _lib.MR_ERR_UNSUPPORTED
