@@ -83,6 +83,15 @@ const char* mr_last_error(void);
 uint64_t mr_kernel_launches(void);
 int mr_abi_version(void);
 
+/* Per-kernel device time, for benchmarks. mr_set_kernel_timing(1) clears the totals and
+ * starts recording a CUDA event pair around every launch of the chain's main kernels (KS,
+ * coherence, EMI) on the launch's stream; (0) stops. mr_kernel_timing synchronises the
+ * recorded events, returns the number of kernels seen and, for 0 <= i < that number, gives
+ * kernel i's name, total milliseconds and launch count. Timing adds an event pair per launch,
+ * so time a separate pass with it, not the headline one. No reference counterpart. */
+void mr_set_kernel_timing(int on);
+int mr_kernel_timing(int i, const char** name, double* total_ms, int64_t* launches);
+
 /* ---------------------------------------------------------------- intensity prologue
  * rmli = re*re + im*im (float32, each product and the sum rounded once): the |slc|^2
  * that the notebooks feed to ks_test (nbs/API/pl.ipynb cell 15, `np.abs(rslc)**2`),

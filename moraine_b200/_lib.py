@@ -29,6 +29,8 @@ _SIGNATURES = {
     "mr_last_error": (ctypes.c_char_p, []),
     "mr_abi_version": (c_int, []),
     "mr_kernel_launches": (ctypes.c_uint64, []),
+    "mr_set_kernel_timing": (None, [c_int]),
+    "mr_kernel_timing": (c_int, [c_int, P, P, P]),
     "mr_gamma_sample_bytes": (c_size_t, [c_int]),
     "mr_set_autotune": (None, [c_int]),
     "mr_ks_plan": (c_int, [c_int, c_int, c_int, P, P, P]),
@@ -98,6 +100,17 @@ def load() -> ctypes.CDLL:
         lib.mr_set_autotune(1)
         _lib = lib
         return _lib
+
+
+def kernel_timing() -> dict:
+    """Per-kernel device time recorded since mr_set_kernel_timing(1): name -> (ms, launches)."""
+    lib = load()
+    name, ms, cnt = ctypes.c_char_p(), ctypes.c_double(), ctypes.c_int64()
+    out = {}
+    for i in range(lib.mr_kernel_timing(-1, None, None, None)):
+        lib.mr_kernel_timing(i, ctypes.byref(name), ctypes.byref(ms), ctypes.byref(cnt))
+        out[name.value.decode()] = (ms.value, cnt.value)
+    return out
 
 
 def last_error() -> str:

@@ -227,6 +227,7 @@ int launch_gram(const float2* rslc, int nlines, int width, int n, const int32_t*
                       (size_t)az_win * r_win * sizeof(int);
   if (int rc = allow_smem(reinterpret_cast<const void*>(gram_kernel<A, kFull>), smem)) return rc;
   const int64_t grid = std::min<int64_t>(n_pc, (int64_t)sm_count() * 8);
+  KernelTimer kt(sizeof(A) == 8 ? "gram fp64" : "gram fp32", s);
   gram_kernel<A, kFull><<<(unsigned)grid, kGramThreads, smem, s>>>(rslc, nlines, width, n, idx, n_pc, mask,
                                                                    mask_stride, az_win, r_win, coh, cov, dcount, doff);
   return check_launch("coherence gram");

@@ -367,6 +367,7 @@ int gram_tc(const float2* rslc, int nlines, int width, int n, const int32_t* idx
   MR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kTcThreads, L.bytes));
   occ = std::max(1, std::min(occ, 512 / L.ncols));
   const int64_t grid = std::min<int64_t>(n_pc, (int64_t)sm_count() * occ);
+  KernelTimer kt(split ? "gram tc bf16x3" : "gram tc bf16", s);
   kern<<<(unsigned)grid, kTcThreads, L.bytes, s>>>(rslc, nlines, width, n, idx, n_pc, mask, mask_stride, az_win,
                                                    r_win, coh);
   return check_launch("coherence gram (tensor cores)");

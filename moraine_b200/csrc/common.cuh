@@ -39,6 +39,23 @@ inline int check_launch(const char* what, int launches = 1) {
 
 inline cudaStream_t as_stream(mr_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Per-kernel device timing for benchmarks (mr_set_kernel_timing): while it is on, an
+// instrumented launch records a CUDA event pair around itself on its stream (never inside
+// a stream capture), and mr_kernel_timing adds them up per kernel name. Off by default;
+// the object does nothing then.
+class KernelTimer {
+ public:
+  KernelTimer(const char* name, cudaStream_t s);
+  ~KernelTimer();
+  KernelTimer(const KernelTimer&) = delete;
+  KernelTimer& operator=(const KernelTimer&) = delete;
+
+ private:
+  const char* name_;
+  cudaStream_t s_;
+  cudaEvent_t e0_ = nullptr;
+};
+
 // Number of SMs of the current device (cached per device).
 int sm_count();
 

@@ -255,6 +255,7 @@ int emi_entry(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, int p
   // N > 128: FP64 throughout
   const size_t smem = sizeof(GeneralShared);
   if (int rc_ = allow_smem(reinterpret_cast<const void*>(general_kernel), (size_t)(smem))) return rc_;
+  KernelTimer kt("emi general fp64", s);
   general_kernel<<<general_grid(n_pc), kThreads, smem, s>>>(c, n_pc, nimages, ref, p, emi_quality, t_coh,
                                                             static_cast<double*>(workspace));
   if (int rc = check_launch("emi")) return rc;

@@ -294,6 +294,7 @@ template <int E>
 void launch_sort(const float* rmli, int64_t npix, int n, uint32_t* keys, cudaStream_t s) {
   int64_t blocks = (npix + 7) / 8;
   int grid = (int)std::min<int64_t>(blocks, (int64_t)sm_count() * 32);
+  KernelTimer kt("ks sort keys", s);
   sort_keys_kernel<E><<<grid, 256, 0, s>>>(rmli, npix, n, keys);
 }
 
@@ -344,6 +345,7 @@ int launch_merge(const KsPlan& plan, const uint32_t* keys, int nlines, int width
   if (int rc = allow_smem(reinterpret_cast<const void*>(ks_merge_kernel), plan.smem)) return rc;
   const int64_t tiles = (int64_t)((nlines + plan.th - 1) / plan.th) * ((width + plan.tw - 1) / plan.tw);
   MR_REQUIRE(tiles < (1ll << 31), "ks_test: image too large");
+  KernelTimer kt("ks merge", s);
   ks_merge_kernel<<<(unsigned)tiles, kKsThreads, plan.smem, s>>>(keys, nlines, width, n, azh, rh, plan.th, plan.tw,
                                                                  plan.azc, plan.ss, tab, p, dist, is_shp, shp_num);
   return check_launch("ks_test merge");

@@ -207,6 +207,18 @@ def emi(coh: np.ndarray, ref: int = 0, chunk: int = 4096):
     return ph, q, gap, cond
 
 
+def emi_c64(coh: np.ndarray, ref: int = 0):
+    """moraine/pl.py:46-65 in the reference's own arithmetic: complex64 / float32 LAPACK
+    (inv of |Gamma|, eigh of M), as the reference's CPU path computes it. The CPU baseline's
+    arm, not a checker: results follow the complex64 rounding, not FP64."""
+    coh = np.asarray(coh, np.complex64)
+    g = uncompress_coh(coh)
+    m = np.linalg.inv(np.abs(g)) * g
+    w, v = np.linalg.eigh(m)
+    v0 = v[..., 0] * v[..., ref, 0].conj()[..., None]
+    return (v0 / np.abs(v0)).astype(np.complex64), w[..., 0].astype(np.float32)
+
+
 def phase_tolerance(cond: np.ndarray, gap: np.ndarray, eps: float, floor: float = 1e-4) -> np.ndarray:
     """Per-point phase tolerance (rad) for a computation with unit roundoff ``eps``."""
     return np.maximum(floor, 4.0 * eps * cond / np.maximum(gap, 1e-12))

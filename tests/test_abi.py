@@ -89,3 +89,11 @@ def test_header_binds_from_plain_c(tmp_path):
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0, (out.returncode, out.stdout, out.stderr)
     assert out.stdout.startswith("ok ") and "ks_test" in out.stdout
+
+
+def test_kernel_timing_empty_without_launches():
+    lib = _lib.load()
+    lib.mr_set_kernel_timing(1)
+    assert _lib.kernel_timing() == {}
+    lib.mr_set_kernel_timing(0)
+    assert lib.mr_kernel_timing(-1, None, None, None) == 0
