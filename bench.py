@@ -52,6 +52,8 @@ def parse():
                                                           "with an fp64 Gram, else fp32)")
     ap.add_argument("--no-variants", action="store_true", help="skip the precision variants")
     ap.add_argument("--no-oracle", action="store_true", help="skip the check against the FP64 oracle")
+    ap.add_argument("--other-configs", default="c1,c3", help="other benchmark scenes run once after the headline "
+                                                             "('' for none)")
     ap.add_argument("--oracle-points", type=int, default=10240, help="DS points checked against the oracle")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -231,6 +233,75 @@ def stage_rooflines(cfg, stage: dict, n_ds: int, res, peaks: dict, fp32: float, 
     return out
 
 
+def kernel_rooflines(cfg, ktimes: dict, n_ds: int, res, peaks: dict, fp32: float) -> dict:
+    """Every timed kernel's average launch against the pipe or memory bound that limits it.
+
+    ``ktimes``: name -> (total ms, launches) from the library's event pairs. Algorithmic work
+    per unit, and the bound:
+      ks sort keys      pixel: 4N bytes in, 4K out (K = keys per pixel)          HBM
+      ks merge          pixel: 4N + W + 4 bytes (keys in, mask and count out)     HBM (as asked;
+                        its real limit is integer issue: W(2N-1) merge steps per pixel)
+      gram fp32/fp64    DS point: 8 S Q + 3 S N flops (S its SHP count)          FP32 / FP64 pipe
+      emi inverse       DS point: N^3/3 + N^3 flops (factorisation and inverse of |Gamma|)
+      emi reduce        DS point: 4N^3/3 flops (the complex factorisation of M)
+      emi tail          DS point: 80 N^2 flops (solves, back-transformation)
+    The EMI split follows the terms of the stage's 2.7 N^3 + 80 N^2 figure; the kernels
+    execute more (2 N^3 for Gauss-Jordan, 16 N^3/3 for the Householder reduction), given as
+    executed_flops_per_unit.
+    """
+    n = cfg.nimages
+    npix = cfg.nlines * cfg.width
+    q = n * (n - 1) // 2
+    w = cfg.az_win * cfg.r_win
+    hbm = peaks.get("hbm_gbs")
+    s_sum = None
+    if n_ds:
+        idx = res.idx.long()
+        s_sum = float(res.shp_num[idx[:, 0], idx[:, 1]].double().sum().item())
+    out = {}
+    for name, (ms, launches) in ktimes.items():
+        if not launches or ms <= 0:
+            continue
+        per = ms / launches
+        ent = {"kernel": name, "launches": launches, "ms_total": ms, "ms_per_launch": per, "traffic": None}
+        if name == "ks sort keys":
+            byts = npix * (4 * n + 4 * ((n + 4) & ~3)) / launches
+            ent.update(bound="hbm", unit="GB/s", achieved=byts / (per / 1e3) / 1e9, peak=hbm,
+                       peak_source=peaks["source"])
+        elif name == "ks merge":
+            byts = npix * (4 * n + w + 4) / launches
+            ent.update(bound="hbm", unit="GB/s", achieved=byts / (per / 1e3) / 1e9, peak=hbm,
+                       peak_source=peaks["source"],
+                       merge_steps_per_s=npix * w * (2 * n - 1) / (ms / 1e3))
+        elif name.startswith("gram") and s_sum is not None and "tc" not in name:
+            flops = (8 * q + 3 * n) * s_sum / launches
+            peak = fp32 / 2 if name.endswith("fp64") else fp32
+            ent.update(bound="fp64-simt" if name.endswith("fp64") else "fp32-simt", unit="TFLOP/s",
+                       achieved=flops / (per / 1e3) / 1e12, peak=peak,
+                       peak_source="cuBLAS SGEMM in this run (FP32, TF32 off)"
+                       + (", halved for the FP64 pipe" if name.endswith("fp64") else ""))
+        elif name.startswith("emi") and n_ds and "rerun" not in name:
+            pts = n_ds / launches
+            if "inverse" in name:
+                alg, exe = 4 * n ** 3 / 3, 2 * n ** 3
+            elif "reduce" in name:
+                alg, exe = 4 * n ** 3 / 3, 16 * n ** 3 / 3
+            else:
+                alg, exe = 80 * n ** 2, None
+            f64 = name.endswith("fp64")
+            peak = fp32 / 2 if f64 else fp32
+            ent.update(bound="fp64-simt" if f64 else "fp32-simt", unit="TFLOP/s",
+                       achieved=alg * pts / (per / 1e3) / 1e12, peak=peak,
+                       peak_source="cuBLAS SGEMM in this run (FP32, TF32 off)"
+                       + (", halved for the FP64 pipe" if f64 else ""),
+                       algorithmic_flops_per_unit=alg, executed_flops_per_unit=exe, units_per_launch=pts)
+        else:
+            continue
+        ent["frac"] = ent["achieved"] / ent["peak"] if ent.get("peak") else None
+        out[name] = ent
+    return out
+
+
 # ----------------------------------------------------------------------------- precision
 def precision_variants(cfg, rslc, ref, dev) -> dict:
     """Time and accuracy of the chain's arithmetic variants against the FP64 chain on the same
@@ -334,6 +405,50 @@ def oracle_check(cfg, rslc, res, gram: str, n_points: int = 10240, nthreads: int
             "nan_points": int((~fin).sum()), "oracle_s": time.perf_counter() - t0,
             "oracle": "C FP64 Gram (stored complex64) + numpy LAPACK eigh/inv FP64 + C temporal coherence, "
                       "DS points drawn evenly over the run"}
+
+
+# ----------------------------------------------------------------------------- other configs
+def config_leg(name: str, dev, gram: str, emi: str, variants, steps: int = 2, oracle_points: int = 2048) -> dict:
+    """One pass of the chain on another benchmark scene (its own size, window and image
+    count), timed after a warm-up pass, and the accuracy of each arithmetic variant against
+    the FP64 oracle on a sample of its DS points (coherence max-abs, phase error, temporal
+    coherence error, share of points recomputed in FP64)."""
+    import torch  # noqa: PLC0415
+
+    from moraine_b200.chain import DsChain  # noqa: PLC0415
+    from moraine_b200.synth import CONFIGS, make_stack  # noqa: PLC0415
+
+    cfg = CONFIGS[name]
+    z = make_stack(cfg, device=dev)
+    out = {"workload": f"ds-chain {cfg.name} {cfg.nlines}x{cfg.width}x{cfg.nimages} complex64, window "
+                       f"{cfg.az_win}x{cfg.r_win}, DS = SHP count >= {cfg.min_shp}", "variants": {}}
+    if cfg.nimages > 128:
+        out["note"] = ("nimages > 128: EMI runs the FP64 kernel for every EMI arithmetic, so only the Gram "
+                       "arithmetic differs between variants; the tensor-core Gram supports nimages <= 128")
+    for g, e in variants:
+        ch = DsChain(cfg.nlines, cfg.width, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp,
+                     precision=g, emi_precision=e, device=dev)
+        r = ch.run(z)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            r = ch.run(z)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        ent = {"ds_pixels_per_s": r.n_ds / (ms / 1e3), "ms_per_step": ms, "n_ds": r.n_ds,
+               "routed_to_fp64": float((r.route == 1).float().mean()) if r.route is not None else
+               (1.0 if e == "fp64" or cfg.nimages > 128 else 0.0)}
+        if oracle_points:
+            ent["oracle_check"] = oracle_check(cfg, z, r, g, n_points=oracle_points)
+        out["variants"][f"gram {g}, emi {e}"] = ent
+        log(f"{name} gram {g} emi {e}: {ent['ds_pixels_per_s']:.0f} DS px/s")
+        del ch, r
+        torch.cuda.empty_cache()
+    if (gram, emi) in variants:
+        out["headline"] = out["variants"][f"gram {gram}, emi {emi}"]["ds_pixels_per_s"]
+    return out
 
 
 # ----------------------------------------------------------------------------- streaming
@@ -557,8 +672,14 @@ def main():
     n_ds = res.n_ds
 
     # per-stage split (separate pass with events, outside the timed region)
+    # per-kernel device time (event pairs around every launch), also a separate pass
+    lib0 = _lib.load()
     chain.timing = True
+    lib0.mr_set_kernel_timing(1)
     stage = chain.run(rslc).stage_ms
+    torch.cuda.synchronize()
+    ktimes = _lib.kernel_timing()
+    lib0.mr_set_kernel_timing(0)
     chain.timing = False
 
     clocks = ClockSampler(local)
@@ -656,10 +777,18 @@ def main():
     fp32 = fp32_simt_peak(dev)
     log(f"FP32 SIMT reference rate: {fp32:.1f} TFLOP/s (cuBLAS SGEMM, TF32 off)")
     stage_roof = stage_rooflines(cfg, stage, n_ds, res, peaks, fp32, chain, args.precision)
-    dom = max(stage_roof, key=lambda k: stage_roof[k]["ms"]) if stage_roof else None
-    roofline = dict(stage_roof[dom]) if dom else None
-    if roofline:
-        roofline["stage"] = dom
+    kernel_roof = kernel_rooflines(cfg, ktimes, n_ds, res, peaks, fp32)
+    dom = max(kernel_roof, key=lambda k: kernel_roof[k]["ms_total"]) if kernel_roof else None
+    roofline = dict(kernel_roof[dom]) if dom else None
+    others = None
+    if args.other_configs and world == 1 and not args.size:
+        others = {}
+        for name in [c for c in args.other_configs.split(",") if c]:
+            log(f"config {name}")
+            var = [("fp32", "fp32"), ("fp64", "fp64"), ("fp64", "refine"), ("fp64", "mixed")]
+            if name == "c3":
+                var = [("fp32", "fp32"), ("fp64", "fp64"), ("fp64", "refine")]
+            others[name] = config_leg(name, dev, args.precision, chain.emi_precision, var)
     latency = None
     if args.serve_requests > 0 and world == 1:
         log(f"serving episode: {args.serve_requests} tiles")
@@ -687,7 +816,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": dtype_of(args.precision, chain.emi_precision), "data": "synthetic",
             "config": workload, "n_ds_per_gpu": n_ds, "stage_ms": stage, "roofline": roofline,
-            "stage_roofline": stage_roof, "precision_variants": variants, "oracle_check": oracle,
+            "stage_roofline": stage_roof, "kernel_roofline": kernel_roof, "kernel_ms": ktimes,
+            "precision_variants": variants, "oracle_check": oracle, "other_configs": others,
             "cpu_baseline": cpu, "e2e": e2e, "scene_stream": stream, "latency": latency, "clocks": clk, "gpu_launches": launches,
         }))
     if world > 1:

@@ -1282,7 +1282,7 @@ int launch_inverse(const float2* coh, PointSet pts, int64_t grid_cap, int n, uns
   constexpr int CX = gj_cx<T>();
   const int occ = std::max(1, occupancy(inverse_kernel<T, NB, CX, TW>, 16 * CX, 0));
   const int64_t grid = std::min<int64_t>(grid_cap, (int64_t)sm_count() * occ);
-  KernelTimer kt(sizeof(T) == 8 ? "emi inverse fp64" : "emi inverse fp32", s);
+  KernelTimer kt(pts.list ? "emi inverse rerun" : sizeof(T) == 8 ? "emi inverse fp64" : "emi inverse fp32", s);
   inverse_kernel<T, NB, CX, TW><<<(unsigned)grid, 16 * CX, 0, s>>>(coh, pts, n, ws, sing, cond_max);
   return check_launch("emi inverse");
 }
@@ -1309,7 +1309,7 @@ int run_reduce(const float2* c, PointSet pts, int n, unsigned char* ws, cudaStre
   if (int rc_ = allow_smem(reinterpret_cast<const void*>(reduce_kernel<T, TA>), (size_t)(rsmem))) return rc_;
   const int rocc = occupancy(reduce_kernel<T, TA>, kThreads, rsmem);
   if (rocc < 1) return fail(MR_ERR_UNSUPPORTED, "emi: %zu bytes of shared memory per CTA do not fit", rsmem);
-  KernelTimer kt(sizeof(T) == 8 ? "emi reduce fp64" : "emi reduce fp32", s);
+  KernelTimer kt(pts.list ? "emi reduce rerun" : sizeof(T) == 8 ? "emi reduce fp64" : "emi reduce fp32", s);
   reduce_kernel<T, TA><<<(unsigned)std::min<int64_t>(pts.n_pc, (int64_t)sm_count() * rocc), kThreads, rsmem, s>>>(
       c, pts, n, ws);
   return check_launch("emi reduce");
@@ -1327,7 +1327,7 @@ int run_pass(const float2* c, PointSet pts, int n, int ref, float2* ph, float* q
   if (int rc_ = allow_smem(reinterpret_cast<const void*>(tail_kernel<T, T>), (size_t)(tsmem))) return rc_;
   const int tocc = std::max(1, occupancy(tail_kernel<T, T>, 32 * kTailWarps, tsmem));
   const int64_t tgrid = std::min<int64_t>((pts.n_pc + kTailWarps - 1) / kTailWarps, (int64_t)sm_count() * tocc);
-  KernelTimer kt(sizeof(T) == 8 ? "emi tail fp64" : "emi tail fp32", s);
+  KernelTimer kt(pts.list ? "emi tail rerun" : sizeof(T) == 8 ? "emi tail fp64" : "emi tail fp32", s);
   tail_kernel<T, T><<<(unsigned)tgrid, 32 * kTailWarps, tsmem, s>>>(c, pts, n, ref, ws, sing, ph, quality, tcoh);
   return check_launch("emi tail");
 }

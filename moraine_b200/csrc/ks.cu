@@ -108,6 +108,15 @@ struct KsPlan {
 
 constexpr int kKsThreads = 256;
 
+// Keys i .. i+3 of a pixel into its shared-memory row (odd stride, so scalar stores); the
+// row holds keys 0..n (key n is the sentinel).
+__device__ __forceinline__ void stage4(uint32_t* dst, int i, uint4 v, int n) {
+  if (i <= n) dst[i] = v.x;
+  if (i + 1 <= n) dst[i + 1] = v.y;
+  if (i + 2 <= n) dst[i + 2] = v.z;
+  if (i + 3 <= n) dst[i + 3] = v.w;
+}
+
 __global__ void __launch_bounds__(kKsThreads) ks_merge_kernel(
     const uint32_t* __restrict__ keys, int nlines, int width, int n, int azh, int rh,
     int th, int tw, int azc, int ss, const __grid_constant__ KsTable tab, float* __restrict__ p,
@@ -134,13 +143,19 @@ __global__ void __launch_bounds__(kKsThreads) ks_merge_kernel(
   const int r0 = (blockIdx.x / tiles_x) * th;
   const int c0 = (blockIdx.x % tiles_x) * tw;
 
-  // reference tile
-  for (int e = threadIdx.x; e < nrp * ks; e += blockDim.x) {
-    int rp = e / ks, i = e - rp * ks;
-    int r = r0 + rp / tw, c = c0 + rp % tw;
-    uint32_t v = kKeyMax;
-    if (r < nlines && c < width) v = keys[((int64_t)r * width + c) * ks + i];
-    if (i <= n) ref_tile[rp * ss + i] = v;
+  // reference tile: a warp per pixel, 16-byte loads (ks is a multiple of 4), no per-key
+  // index arithmetic
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int kq = ks >> 2;
+  for (int rp = wid; rp < nrp; rp += nw) {
+    const int r = r0 + rp / tw, c = c0 + rp % tw;
+    uint32_t* dst = ref_tile + rp * ss;
+    if (r < nlines && c < width) {
+      const uint4* src = reinterpret_cast<const uint4*>(keys + ((int64_t)r * width + c) * ks);
+      for (int q = lane; q < kq; q += 32) stage4(dst, 4 * q, __ldg(src + q), n);
+    } else {
+      for (int i = lane; i <= n; i += 32) dst[i] = kKeyMax;
+    }
   }
   if (threadIdx.x < nrp) s_cnt[threadIdx.x] = 0;
   __syncthreads();
@@ -157,12 +172,15 @@ __global__ void __launch_bounds__(kKsThreads) ks_merge_kernel(
     const int hrows = th + nz - 1;
     __syncthreads();  // previous chunk done with the halo
     // halo rows: image rows r0 - azh + z0 .. + hrows-1, cols c0 - rh .. + hw-1
-    for (int e = threadIdx.x; e < hrows * hw * ks; e += blockDim.x) {
-      int hp = e / ks, i = e - hp * ks;
-      int r = r0 - azh + z0 + hp / hw, c = c0 - rh + hp % hw;
-      uint32_t v = kKeyMax;
-      if (r >= 0 && r < nlines && c >= 0 && c < width) v = keys[((int64_t)r * width + c) * ks + i];
-      if (i <= n) halo[hp * ss + i] = v;
+    for (int hp = wid; hp < hrows * hw; hp += nw) {
+      const int r = r0 - azh + z0 + hp / hw, c = c0 - rh + hp % hw;
+      uint32_t* dst = halo + hp * ss;
+      if (r >= 0 && r < nlines && c >= 0 && c < width) {
+        const uint4* src = reinterpret_cast<const uint4*>(keys + ((int64_t)r * width + c) * ks);
+        for (int q = lane; q < kq; q += 32) stage4(dst, 4 * q, __ldg(src + q), n);
+      } else {
+        for (int i = lane; i <= n; i += 32) dst[i] = kKeyMax;
+      }
     }
     __syncthreads();
     if (ref_in) {
