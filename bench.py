@@ -48,8 +48,9 @@ def parse():
     ap.add_argument("--config", default="c2")
     ap.add_argument("--size", type=int, default=0, help="override nlines = width (smaller runs)")
     ap.add_argument("--precision", default="fp64", help="coherence Gram arithmetic: fp64, fp32, bf16x3, bf16")
-    ap.add_argument("--emi-precision", default=None, help="EMI arithmetic: fp64, fp32 or mixed (default: fp64 "
-                                                          "with an fp64 Gram, else fp32)")
+    ap.add_argument("--emi-precision", default=None,
+                    help="EMI arithmetic: fp64, fp32, mixed or refine (default: refine with an fp64 Gram - FP64 "
+                         "inverse, FP32 reduction, FP64 refinement and check - else fp32)")
     ap.add_argument("--no-variants", action="store_true", help="skip the precision variants")
     ap.add_argument("--no-oracle", action="store_true", help="skip the check against the FP64 oracle")
     ap.add_argument("--other-configs", default="c1,c3", help="other benchmark scenes run once after the headline "
@@ -656,8 +657,10 @@ def main():
     rslc = make_stack(rcfg, device=dev)
     torch.cuda.synchronize()
     log("stack ready")
+    emi_prec = args.emi_precision or ("refine" if args.precision == "fp64" else None)
+    args.emi_precision = emi_prec  # the serving episode and the streamed scene use the same EMI
     chain = DsChain(cfg.nlines, cfg.width, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp,
-                    precision=args.precision, emi_precision=args.emi_precision, device=dev)
+                    precision=args.precision, emi_precision=emi_prec, device=dev)
     workload["emi_precision"] = chain.emi_precision
 
     def barrier():
