@@ -646,10 +646,12 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 2) reduce_kerne
     PointPtr<T, TA> w(ws, pt, n);
     // M = inv(|Gamma|) o Gamma: read along the upper triangle (inverse and coherence both
     // contiguous), written to the packed lower triangle as M_jm = conj(M_mj)
+    // row m of element q: rows start at tri_up(m, m, n), which grows only up to m = n, so the
+    // walk stops at the last row
     int m = 0;
-    while (tri_up(m + 1, m + 1, n) <= tid) ++m;
+    while (m + 1 < n && tri_up(m + 1, m + 1, n) <= tid) ++m;
     for (int q = tid; q < np; q += nt) {
-      while (tri_up(m + 1, m + 1, n) <= q) ++m;
+      while (m + 1 < n && tri_up(m + 1, m + 1, n) <= q) ++m;
       const int j = m + (q - (int)tri_up(m, m, n));
       const TA sc = w.ainv[q];
       T gx = 1, gy = 0;
