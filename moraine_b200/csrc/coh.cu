@@ -62,12 +62,11 @@ __device__ int collect_shps(const uint8_t* __restrict__ mask, int az_win, int r_
   return total;
 }
 
-// One CTA per point (grid-stride). Each thread accumulates a BM x BM block of the N x N
-// Gram over the point's SHPs, staged kChunk rows at a time in shared memory in the
-// accumulation arithmetic A (converted once when staged, not in the inner loop).
+// One CTA per point (grid-stride). Each thread accumulates a 4x4 block of the N x N
+// Gram over the point's SHPs, staged kChunk rows at a time in shared memory.
 // kFull = false: upper-triangle blocks, writes coh (n_pc, Q) in triu order.
 // kFull = true : all blocks, writes cov and coh (npix, N, N) (raster form).
-template <typename A, bool kFull, int BM>
+template <typename A, bool kFull>
 __global__ void __launch_bounds__(kGramThreads) gram_kernel(
     const float2* __restrict__ rslc, int nlines, int width, int n, const int32_t* __restrict__ idx,
     int64_t n_pc, const uint8_t* __restrict__ mask, int mask_stride, int az_win, int r_win,
@@ -79,12 +78,12 @@ __global__ void __launch_bounds__(kGramThreads) gram_kernel(
   }
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int win = az_win * r_win;
-  const int npad = (n + BM - 1) / BM * BM;
-  C* zc = reinterpret_cast<C*>(smem_raw);                             // kChunk x npad
+  const int npad = (n + 3) & ~3;
+  float2* zc = reinterpret_cast<float2*>(smem_raw);                  // kChunk x npad
   A* amp2 = reinterpret_cast<A*>(zc + kChunk * npad);                 // npad
   int* s_pos = reinterpret_cast<int*>(amp2 + npad);                   // win
   __shared__ int s_tmp[33];
-  const int nb = npad / BM;
+  const int nb = npad / 4;
   const int nblk = kFull ? nb * nb : nb * (nb + 1) / 2;
   const int64_t npairs = (int64_t)n * (n - 1) / 2;
 
@@ -126,11 +125,11 @@ __global__ void __launch_bounds__(kGramThreads) gram_kernel(
           bj = bm + b;
         }
       }
-      C acc[BM][BM];
+      C acc[4][4];
 #pragma unroll
-      for (int a = 0; a < BM; ++a)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < BM; ++b) { acc[a][b].x = 0; acc[a][b].y = 0; }
+        for (int b = 0; b < 4; ++b) { acc[a][b].x = 0; acc[a][b].y = 0; }
       for (int s0 = 0; s0 < S; s0 += kChunk) {
         const int ns = min(kChunk, S - s0);
         __syncthreads();
@@ -138,35 +137,33 @@ __global__ void __launch_bounds__(kGramThreads) gram_kernel(
           int t = e / npad, c = e - t * npad;
           float2 z = make_float2(0.f, 0.f);
           if (c < n) z = rslc[(int64_t)s_pos[s0 + t] * n + c];
-          C zz;
-          zz.x = (A)z.x;
-          zz.y = (A)z.y;
-          zc[t * npad + c] = zz;
+          zc[t * npad + c] = z;
         }
         __syncthreads();
         if (active) {
           for (int t = 0; t < ns; ++t) {
-            const C* row = zc + t * npad;
-            C zm[BM], zj[BM];
+            const float4* row = reinterpret_cast<const float4*>(zc + t * npad);
+            float4 ma = row[2 * bm], mb = row[2 * bm + 1];
+            float4 ja = row[2 * bj], jb = row[2 * bj + 1];
+            const A zm[4][2] = {{ma.x, ma.y}, {ma.z, ma.w}, {mb.x, mb.y}, {mb.z, mb.w}};
+            const A zj[4][2] = {{ja.x, ja.y}, {ja.z, ja.w}, {jb.x, jb.y}, {jb.z, jb.w}};
 #pragma unroll
-            for (int a = 0; a < BM; ++a) { zm[a] = row[BM * bm + a]; zj[a] = row[BM * bj + a]; }
+            for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int a = 0; a < BM; ++a)
-#pragma unroll
-              for (int b = 0; b < BM; ++b) {
+              for (int b = 0; b < 4; ++b) {
                 // z_m * conj(z_j)
-                acc[a][b].x += zm[a].x * zj[b].x + zm[a].y * zj[b].y;
-                acc[a][b].y += zm[a].y * zj[b].x - zm[a].x * zj[b].y;
+                acc[a][b].x += zm[a][0] * zj[b][0] + zm[a][1] * zj[b][1];
+                acc[a][b].y += zm[a][1] * zj[b][0] - zm[a][0] * zj[b][1];
               }
           }
         }
       }
       if (active) {
 #pragma unroll
-        for (int a = 0; a < BM; ++a)
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int b = 0; b < BM; ++b) {
-            const int mm = BM * bm + a, jj = BM * bj + b;
+          for (int b = 0; b < 4; ++b) {
+            const int mm = 4 * bm + a, jj = 4 * bj + b;
             if (mm >= n || jj >= n) continue;
             A den = sqrt(amp2[mm] * amp2[jj]);
             if (kFull) {
@@ -221,46 +218,19 @@ __global__ void gram_pairs_kernel(const float2* __restrict__ rslc, int nlines, i
   }
 }
 
-template <typename A, bool kFull, int BM>
-int launch_gram_bm(const float2* rslc, int nlines, int width, int n, const int32_t* idx, int64_t n_pc,
-                   const uint8_t* mask, int mask_stride, int az_win, int r_win, float2* coh, float2* cov,
-                   cudaStream_t s, const int64_t* dcount, int64_t doff) {
-  using C = typename Acc2<A>::type;
-  const int npad = (n + BM - 1) / BM * BM;
-  const size_t smem = (size_t)kChunk * npad * sizeof(C) + npad * sizeof(A) + (size_t)az_win * r_win * sizeof(int);
-  if (int rc = allow_smem(reinterpret_cast<const void*>(gram_kernel<A, kFull, BM>), smem)) return rc;
-  const int64_t grid = std::min<int64_t>(n_pc, (int64_t)sm_count() * 8);
-  KernelTimer kt(sizeof(A) == 8 ? "gram fp64" : "gram fp32", s);
-  gram_kernel<A, kFull, BM><<<(unsigned)grid, kGramThreads, smem, s>>>(rslc, nlines, width, n, idx, n_pc, mask,
-                                                                       mask_stride, az_win, r_win, coh, cov, dcount,
-                                                                       doff);
-  return check_launch("coherence gram");
-}
-
-// Block side of the Gram's thread tiles: the one (4 or 5) with the least work per thread,
-// rounds of kGramThreads blocks times the block's products (5 x 5 takes the N = 100
-// triangle in one round where 4 x 4 needs two).
-inline int gram_bm(int n, bool full) {
-  int best = 4;
-  long best_cost = 0;
-  for (int bm = 4; bm <= 5; ++bm) {
-    const long nb = (n + bm - 1) / bm;
-    const long blocks = full ? nb * nb : nb * (nb + 1) / 2;
-    const long cost = (blocks + kGramThreads - 1) / kGramThreads * bm * bm;
-    if (bm == 4 || cost < best_cost) { best = bm; best_cost = cost; }
-  }
-  return best;
-}
-
 template <typename A, bool kFull>
 int launch_gram(const float2* rslc, int nlines, int width, int n, const int32_t* idx, int64_t n_pc,
                 const uint8_t* mask, int mask_stride, int az_win, int r_win, float2* coh, float2* cov,
                 cudaStream_t s, const int64_t* dcount = nullptr, int64_t doff = 0) {
-  if (gram_bm(n, kFull) == 5)
-    return launch_gram_bm<A, kFull, 5>(rslc, nlines, width, n, idx, n_pc, mask, mask_stride, az_win, r_win, coh, cov,
-                                       s, dcount, doff);
-  return launch_gram_bm<A, kFull, 4>(rslc, nlines, width, n, idx, n_pc, mask, mask_stride, az_win, r_win, coh, cov, s,
-                                     dcount, doff);
+  const int npad = (n + 3) & ~3;
+  const size_t smem = (size_t)kChunk * npad * sizeof(float2) + npad * sizeof(A) +
+                      (size_t)az_win * r_win * sizeof(int);
+  if (int rc = allow_smem(reinterpret_cast<const void*>(gram_kernel<A, kFull>), smem)) return rc;
+  const int64_t grid = std::min<int64_t>(n_pc, (int64_t)sm_count() * 8);
+  KernelTimer kt(sizeof(A) == 8 ? "gram fp64" : "gram fp32", s);
+  gram_kernel<A, kFull><<<(unsigned)grid, kGramThreads, smem, s>>>(rslc, nlines, width, n, idx, n_pc, mask,
+                                                                   mask_stride, az_win, r_win, coh, cov, dcount, doff);
+  return check_launch("coherence gram");
 }
 
 }  // namespace

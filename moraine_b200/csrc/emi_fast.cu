@@ -40,9 +40,8 @@ struct GjGrid {
 
 template <typename T, int NB, int CX>
 struct GjShared {
-  T col[2][16 * NB];  // pivot column of the next step, by step parity
-  T rp[2];            // its pivot's reciprocal
-  int piv[2];         // its pivot row
+  T col[2][16 * NB];
+  int piv[2];
   int piv_of_step[16 * NB];
   int step_of_row[16 * NB];
   T part[GjGrid<NB, CX>::kWarps][16 * NB];  // row sums of |a| per warp (norm estimate)
@@ -109,60 +108,39 @@ __device__ __forceinline__ void load_abs_gamma(T (&a)[NB][GjGrid<NB, CX>::NC], u
 __device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double recip(double x) { return __drcp_rn(x); }  // = 1.0 / x, IEEE round-to-nearest
 
-// Pivot search key of candidate row `row` (< 128) with value v: the largest key is the row
-// with the largest |v| to 15 bits of mantissa (ties to the smaller row); NaN ranks below
-// every number and above the rows already used (key 0).
-template <typename T> __device__ __forceinline__ unsigned pivot_key(T v, int row, bool eligible) {
-  const float a = fabsf((float)v);
-  const unsigned hi = (a == a) ? (__float_as_uint(a) >> 8) + 1u : 0u;
-  return eligible ? (hi << 8) | 128u | (127u - (unsigned)row) : 0u;
-}
-
-// Bring column SLOT of the half-warp's register tile up to date (a -= f_i r, as the step
-// does everywhere) and publish it as the pivot column of the next step, with its pivot
-// (largest |a| among the rows not used yet) and the pivot's reciprocal. Called by the 16
-// lanes of one column group; `col` holds f (the step's pivot column).
-template <typename T, int NB, int CX, int SLOT>
-__device__ __forceinline__ void gj_publish(T (&a)[NB][GjGrid<NB, CX>::NC], const T* col, T r, int p, T pv,
-                                           unsigned used, int ty, int buf, GjShared<T, NB, CX>& s) {
-  unsigned best = 0;
-#pragma unroll
-  for (int ib = 0; ib < NB; ++ib) {
-    const int i = ty + 16 * ib;
-    const T fi = (i == p) ? pv - T(1) : (col ? col[i] : T(0));
-    a[ib][SLOT] -= fi * r;
-    s.col[buf][i] = a[ib][SLOT];
-    best = max(best, pivot_key(a[ib][SLOT], i, !(used & (1u << ib))));
-  }
-  const unsigned half = (threadIdx.x & 16) ? 0xFFFF0000u : 0x0000FFFFu;
-  best = __reduce_max_sync(half, best);
-  const int p1 = min(127 - (int)(best & 127u), 16 * NB - 1);  // an unused row exists: best >= 128
-  if (ty == (p1 & 15)) {
-    T v = a[0][SLOT];
-#pragma unroll
-    for (int q = 1; q < NB; ++q) v = ((p1 >> 4) == q) ? a[q][SLOT] : v;
-    s.piv[buf] = p1;
-    s.rp[buf] = recip(v);
-  }
-}
-
 // One Gauss-Jordan step k = CX KB + kt on the register tile; KB is a compile-time column
 // slot, so the pivot column is read and rewritten without dynamic register indexing.
-// Look-ahead: the column group owning column k + 1 first brings that column up to date
-// and publishes it with its pivot and reciprocal (gj_publish), then does the rest of its
-// update; the step's other threads only read what the previous step published. One
-// barrier per step.
 template <typename T, int NB, int CX, int KB>
-__device__ __forceinline__ void gj_step(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned& used, int k, int n, int tx,
-                                        int ty, bool& singular, GjShared<T, NB, CX>& s) {
+__device__ __forceinline__ void gj_step(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned& used, int k, int tx, int ty,
+                                        bool& singular, GjShared<T, NB, CX>& s) {
   constexpr int NC = GjGrid<NB, CX>::NC;
-  constexpr int KB1 = KB + 1 < NC ? KB + 1 : 0;
   const int tid = threadIdx.x;
   const int buf = k & 1;
+  const bool owner = tx == (k % CX);
+  if (owner) {  // the half-warp owning column k: publish it, find the pivot
+    const unsigned half = (tx & 1) ? 0xFFFF0000u : 0x0000FFFFu;
+    T best = T(-1);
+    int bi = -1;
+#pragma unroll
+    for (int ib = 0; ib < NB; ++ib) {
+      const T v = a[ib][KB];
+      s.col[buf][ty + 16 * ib] = v;
+      const T av = fabs(v) == fabs(v) ? fabs(v) : T(-0.5);  // NaN ranks last but is taken
+      if (!(used & (1u << ib)) && av > best) { best = av; bi = ty + 16 * ib; }
+    }
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+      const T ob = __shfl_xor_sync(half, best, o, 16);
+      const int oi = __shfl_xor_sync(half, bi, o, 16);
+      if (ob > best || (ob == best && oi >= 0 && (bi < 0 || oi < bi))) { best = ob; bi = oi; }
+    }
+    if (ty == 0) s.piv[buf] = bi;
+  }
+  __syncthreads();
   const int p = s.piv[buf];
   T pv = s.col[buf][p];
-  T rp = s.rp[buf];
-  if (pv == T(0)) { singular = true; pv = T(1); rp = T(1); }
+  if (pv == T(0)) { singular = true; pv = T(1); }
+  const T rp = recip(pv);
   if (ty == (p & 15)) used |= 1u << (p >> 4);
   if (tid == 0) { s.piv_of_step[k] = p; s.step_of_row[p] = k; }
   const int pl = p & 15;
@@ -180,30 +158,17 @@ __device__ __forceinline__ void gj_step(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned
     default: MR_GJ_ROW(7)
 #undef MR_GJ_ROW
   }
-  // look-ahead: column k + 1 sits in slot KB of the next column group, or in slot KB + 1 of
-  // group 0 when k + 1 is a multiple of CX
-  const int k1 = k + 1;
-  const bool wrap = (k1 % CX) == 0;
-  const bool la = k1 < n && tx == k1 % CX && (!wrap || KB + 1 < NC);
-  const int la_slot = la ? (wrap ? KB1 : KB) : -1;
-  if (la) {
-    if (!wrap) gj_publish<T, NB, CX, KB>(a, s.col[buf], r[KB], p, pv, used, ty, buf ^ 1, s);
-    else gj_publish<T, NB, CX, KB1>(a, s.col[buf], r[KB1], p, pv, used, ty, buf ^ 1, s);
-  }
-  // a -= f_i r_j everywhere (the look-ahead column is done), with f_p = pv - 1 so that the
-  // pivot row becomes r; then column k becomes delta_ip / pv - f_i / pv
-  const bool owner = tx == (k % CX);
+  // a -= f_i r_j everywhere, with f_p = pv - 1 so that the pivot row becomes r; then
+  // column k becomes delta_ip / pv - f_i / pv
 #pragma unroll
   for (int ib = 0; ib < NB; ++ib) {
     const int i = ty + 16 * ib;
-    const T f = s.col[buf][i];
-    const T fi = (i == p) ? pv - T(1) : f;
+    const T fi = s.col[buf][i];
+    const T f = (i == p) ? pv - T(1) : fi;
 #pragma unroll
-    for (int jb = 0; jb < NC; ++jb)
-      if (jb != la_slot) a[ib][jb] -= fi * r[jb];
-    if (owner) a[ib][KB] = (i == p) ? rp : -f * rp;
+    for (int jb = 0; jb < NC; ++jb) a[ib][jb] -= f * r[jb];
+    if (owner) a[ib][KB] = (i == p) ? rp : -fi * rp;
   }
-  __syncthreads();
 }
 
 // In-place Gauss-Jordan inverse with partial pivoting on the register tile. Returns true
@@ -213,23 +178,20 @@ __device__ bool gj_tile(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned used, int n, in
                         GjShared<T, NB, CX>& s) {
   constexpr int NC = GjGrid<NB, CX>::NC;
   bool singular = false;
-  // column 0 and its pivot, published by column group 0
-  if (tx == 0) gj_publish<T, NB, CX, 0>(a, nullptr, T(0), -1, T(1), used, ty, 0, s);
-  __syncthreads();
-#pragma unroll 1
+#pragma unroll
   for (int kb = 0; kb < NC; ++kb) {
     for (int kt = 0; kt < CX; ++kt) {
       const int k = CX * kb + kt;
       if (k >= n) break;
-      switch (kb) {  // compile-time slot for each kb
-        case 0: gj_step<T, NB, CX, 0>(a, used, k, n, tx, ty, singular, s); break;
-        case 1: if (NC > 1) gj_step<T, NB, CX, (1 < NC ? 1 : 0)>(a, used, k, n, tx, ty, singular, s); break;
-        case 2: if (NC > 2) gj_step<T, NB, CX, (2 < NC ? 2 : 0)>(a, used, k, n, tx, ty, singular, s); break;
-        case 3: if (NC > 3) gj_step<T, NB, CX, (3 < NC ? 3 : 0)>(a, used, k, n, tx, ty, singular, s); break;
-        case 4: if (NC > 4) gj_step<T, NB, CX, (4 < NC ? 4 : 0)>(a, used, k, n, tx, ty, singular, s); break;
-        case 5: if (NC > 5) gj_step<T, NB, CX, (5 < NC ? 5 : 0)>(a, used, k, n, tx, ty, singular, s); break;
-        case 6: if (NC > 6) gj_step<T, NB, CX, (6 < NC ? 6 : 0)>(a, used, k, n, tx, ty, singular, s); break;
-        default: if (NC > 7) gj_step<T, NB, CX, (7 < NC ? 7 : 0)>(a, used, k, n, tx, ty, singular, s); break;
+      switch (kb) {  // compile-time slot (the loop over kb is unrolled)
+        case 0: gj_step<T, NB, CX, 0>(a, used, k, tx, ty, singular, s); break;
+        case 1: if (NC > 1) gj_step<T, NB, CX, (1 < NC ? 1 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 2: if (NC > 2) gj_step<T, NB, CX, (2 < NC ? 2 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 3: if (NC > 3) gj_step<T, NB, CX, (3 < NC ? 3 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 4: if (NC > 4) gj_step<T, NB, CX, (4 < NC ? 4 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 5: if (NC > 5) gj_step<T, NB, CX, (5 < NC ? 5 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 6: if (NC > 6) gj_step<T, NB, CX, (6 < NC ? 6 : 0)>(a, used, k, tx, ty, singular, s); break;
+        default: if (NC > 7) gj_step<T, NB, CX, (7 < NC ? 7 : 0)>(a, used, k, tx, ty, singular, s); break;
       }
     }
   }
@@ -238,24 +200,24 @@ __device__ bool gj_tile(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned used, int n, in
 }
 
 // ----------------------------------------------------------------- packed reduction
-// Shared memory of the reduction (n = nimages):
-//   L    packed lower triangle of M by rows, (i, j <= i) at tri(i) + j
-//   vec  [2][n] reflectors u_k and u_{k-1}, by step parity
-//   wp   [n]    w_{k-1} of the pending rank-2 update
-//   rowp [n]    row part of the product of the last step, one value per row
-//   cp   [kWarps][n] column part of that product, one partial per warp
-//   d, tau [n], e [n] the tridiagonal and the reflector scalars
 template <typename T>
 struct TriShared {
   using C = typename C2<T>::type;
-  C* L;
-  C* vec;
-  C* wp;
-  C* rowp;
-  C* cp;
+  C* L;       // lower triangle, packed by rows: (i, j <= i) at i(i+1)/2 + j
+  C* pv;      // [2][n] products of the last two steps
+  C* vec;     // [3][n]: u_k and u_{k-1} (by step parity), w_{k-1}
   C* e;
+  C* z;
+  double2* phs;
   T* d;
   T* tau;
+  T* b;
+  T* b2;
+  T* y;
+  T* w1;
+  T* w2;
+  T* w3;
+  Red* red;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -265,24 +227,40 @@ template <typename T>
 __host__ __device__ inline size_t tri_bytes(int n) {
   using C = typename C2<T>::type;
   size_t o = align16((size_t)n * (n + 1) / 2 * sizeof(C));
-  o += align16((size_t)(2 + 1 + 1 + kWarps + 1) * n * sizeof(C));
-  o += align16(2 * (size_t)n * sizeof(T));
-  return o;
+  o = align16(o + 2 * (size_t)n * sizeof(C));
+  o = align16(o + 3 * (size_t)n * sizeof(C));
+  o = align16(o + 2 * (size_t)n * sizeof(C));
+  o = align16(o + (size_t)n * sizeof(double2));
+  o = align16(o + 8 * (size_t)n * sizeof(T));
+  return o + sizeof(Red);
 }
 
 template <typename T>
 __device__ inline TriShared<T> tri_layout(unsigned char* base, int n) {
   using C = typename C2<T>::type;
   TriShared<T> s;
-  s.L = reinterpret_cast<C*>(base);
-  C* v = reinterpret_cast<C*>(base + align16((size_t)n * (n + 1) / 2 * sizeof(C)));
-  s.vec = v;
-  s.wp = v + 2 * n;
-  s.rowp = v + 3 * n;
-  s.cp = v + 4 * n;
-  s.e = v + (4 + kWarps) * n;
-  s.d = reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(v) + align16((size_t)(5 + kWarps) * n * sizeof(C)));
+  size_t o = 0;
+  s.L = reinterpret_cast<C*>(base + o);
+  o = align16(o + (size_t)n * (n + 1) / 2 * sizeof(C));
+  s.pv = reinterpret_cast<C*>(base + o);
+  o = align16(o + 2 * (size_t)n * sizeof(C));
+  s.vec = reinterpret_cast<C*>(base + o);
+  o = align16(o + 3 * (size_t)n * sizeof(C));
+  s.e = reinterpret_cast<C*>(base + o);
+  s.z = s.e + n;
+  o = align16(o + 2 * (size_t)n * sizeof(C));
+  s.phs = reinterpret_cast<double2*>(base + o);
+  o = align16(o + (size_t)n * sizeof(double2));
+  s.d = reinterpret_cast<T*>(base + o);
   s.tau = s.d + n;
+  s.b = s.tau + n;
+  s.b2 = s.b + n;
+  s.y = s.b2 + n;
+  s.w1 = s.y + n;
+  s.w2 = s.w1 + n;
+  s.w3 = s.w2 + n;
+  o = align16(o + 8 * (size_t)n * sizeof(T));
+  s.red = reinterpret_cast<Red*>(base + o);
   return s;
 }
 
@@ -291,6 +269,172 @@ template <typename C> __device__ __forceinline__ void rank2(C& a, C ui, C wj, C 
   a.x -= ui.x * wj.x + ui.y * wj.y + wi.x * uj.x + wi.y * uj.y;
   a.y -= ui.y * wj.x - ui.x * wj.y + wi.y * uj.x - wi.x * uj.y;
 }
+
+// Householder reduction of the Hermitian M (lower triangle, packed in s.L) to tridiagonal
+// (s.d, s.e); reflector k stored in column k (rows k+1..n-1) with scalar s.tau[k]. Whole
+// CTA, three barriers per step:
+//   1. warp 0 finishes step k-1 (w = p - K u, K = tau/2 u^H p) and forms reflector k from
+//      column k brought up to date, x_i = A_i + K B_i, with A_i and B_i computed in the same
+//      pass as the dot product (one load pass, two warp reductions);
+//   2. phase 1: step k-1's rank-2 update on the lower triangle of rows >= k+1 and the row
+//      part of (M u_k)_i = sum_{j<=i} M_ij u_j;
+//   3. phase 2: the column part sum_{j>i} conj(M_ji) u_j, then p_k = tau_k M u_k.
+// Rows are handled in mirrored pairs (i, n+k-i) by groups of 4 to 32 threads (as many as
+// keep the CTA busy while the trailing matrix shrinks), which gives every thread of a step
+// the same number of elements in both phases. The packed triangle halves the
+// shared memory of full storage, so twice as many points are in flight per SM.
+template <typename T>
+__device__ void tridiag_packed(const TriShared<T>& s, int n) {
+  using C = typename C2<T>::type;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  C* L = s.L;
+  C* wp = s.vec + 2 * n;  // w_{k-1}
+  for (int k = 0; k + 2 < n; ++k) {
+    C* up = s.vec + ((k + 1) & 1) * n;  // u_{k-1}
+    C* uc = s.vec + (k & 1) * n;        // u_k
+    // ---- warp 0: finish step k-1 and form reflector k
+    if (wid == 0) {
+      const T tau_prev = k > 0 ? s.tau[k - 1] : T(0);
+      const bool pending = tau_prev != T(0);
+      const C* p = s.pv + ((k + 1) & 1) * n;
+      C A[4], B[4], pp[4], uu[4];
+      T dot = 0;
+      C pk = mk<T>(0, 0), ukk = mk<T>(0, 0);
+      if (pending) { pk = p[k]; ukk = up[k]; }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int i = k + lane + 32 * t;
+        A[t] = B[t] = pp[t] = uu[t] = mk<T>(0, 0);
+        if (i < n) {
+          const int base = tri(i);
+          A[t] = L[base + k];
+          if (pending) {
+            pp[t] = p[i];
+            uu[t] = up[i];
+            dot += uu[t].x * pp[t].x + uu[t].y * pp[t].y;
+            // x_i = a_ik - u_i conj(w_k) - w_i conj(u_k) = A_i + K B_i, w = p - K u
+            rank2(A[t], uu[t], pk, pp[t], ukk);
+            B[t] = mk<T>(2 * (uu[t].x * ukk.x + uu[t].y * ukk.y), 2 * (uu[t].y * ukk.x - uu[t].x * ukk.y));
+            L[base + k - 1] = uu[t];  // reflector k-1 (rows >= k) kept in column k-1
+          }
+        }
+      }
+      const T K = pending ? T(0.5) * tau_prev * warp_sum(dot) : T(0);
+      T xn2 = 0;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int i = k + lane + 32 * t;
+        if (i < n) {
+          const C x = mk<T>(A[t].x + K * B[t].x, A[t].y + K * B[t].y);
+          if (pending) wp[i] = mk<T>(pp[t].x - K * uu[t].x, pp[t].y - K * uu[t].y);
+          uc[i] = x;
+          if (i >= k + 2) xn2 += x.x * x.x + x.y * x.y;
+        }
+      }
+      xn2 = warp_sum(xn2);
+      __syncwarp();
+      const C alpha = uc[k + 1];
+      T tau_k = 0;
+      C ek = alpha;
+      if (xn2 != T(0)) {
+        const T aa = sqrt(alpha.x * alpha.x + alpha.y * alpha.y);
+        const T nrm = sqrt(aa * aa + xn2);
+        const C ph1 = aa > T(0) ? mk<T>(alpha.x / aa, alpha.y / aa) : mk<T>(1, 0);
+        tau_k = T(2) / ((aa + nrm) * (aa + nrm) + xn2);
+        ek = mk<T>(-ph1.x * nrm, -ph1.y * nrm);
+        if (lane == 0) uc[k + 1] = mk<T>(ph1.x * (aa + nrm), ph1.y * (aa + nrm));
+      }
+      if (lane == 0) { s.d[k] = uc[k].x; s.e[k] = ek; s.tau[k] = tau_k; }
+    }
+    __syncthreads();
+    const bool pending = k > 0 && s.tau[k - 1] != T(0);
+    const T tau_k = s.tau[k];
+    const int m = n - k - 1;         // rows k+1..n-1
+    const int npair = (m + 1) >> 1;  // mirrored pairs (the middle row of an odd m alone)
+    // G threads per pair, as many as keep every thread of the CTA busy (4 to 32)
+    int G = 4;
+    while (G < 32 && npair * G * 2 <= (int)blockDim.x) G <<= 1;
+    const int pq = tid / G, sub = tid & (G - 1);
+    const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u) << (lane & ~(G - 1));
+    const bool active = (pending || tau_k != T(0)) && pq < npair;
+    const int i1 = k + 1 + pq, i2 = n - 1 - pq;
+    const bool two = i2 != i1;
+    // ---- phase 1: update the lower rows, row part of M u
+    C rs1 = mk<T>(0, 0), rs2 = mk<T>(0, 0);
+    if (active) {
+#pragma unroll 1
+      for (int r = 0; r < 2; ++r) {
+        if (r && !two) break;
+        const int i = r ? i2 : i1;
+        C* row = L + tri(i);
+        C upi = mk<T>(0, 0), wpi = mk<T>(0, 0);
+        if (pending) { upi = up[i]; wpi = wp[i]; }
+        C acc = mk<T>(0, 0);
+        for (int j = k + 1 + sub; j <= i; j += G) {
+          C a = row[j];
+          if (pending) { rank2(a, upi, wp[j], wpi, up[j]); row[j] = a; }
+          const C u = uc[j];
+          acc.x += a.x * u.x - a.y * u.y;
+          acc.y += a.x * u.y + a.y * u.x;
+        }
+        if (r) rs2 = acc; else rs1 = acc;
+      }
+    }
+    __syncthreads();
+    // ---- phase 2: column part, then p_k
+    if (active && tau_k != T(0)) {
+#pragma unroll 1
+      for (int r = 0; r < 2; ++r) {
+        if (r && !two) break;
+        const int i = r ? i2 : i1;
+        C acc = r ? rs2 : rs1;
+        for (int j = i + 1 + sub; j < n; j += G) {
+          const C a = L[tri(j) + i];  // M_ji, lower triangle
+          const C u = uc[j];
+          acc.x += a.x * u.x + a.y * u.y;  // conj(M_ji) u_j
+          acc.y += a.x * u.y - a.y * u.x;
+        }
+        for (int o = 1; o < G; o <<= 1) {
+          acc.x += __shfl_xor_sync(gmask, acc.x, o);
+          acc.y += __shfl_xor_sync(gmask, acc.y, o);
+        }
+        if (sub == 0) s.pv[(k & 1) * n + i] = mk<T>(tau_k * acc.x, tau_k * acc.y);
+      }
+    }
+    __syncthreads();
+  }
+  // last pending update (step n-3) on the trailing 2 x 2 block; reflector n-3 stored
+  if (wid == 0) {
+    if (n >= 3 && s.tau[n - 3] != T(0)) {
+      const T tau_prev = s.tau[n - 3];
+      const C* up = s.vec + ((n - 3) & 1) * n;
+      const C* p = s.pv + ((n - 3) & 1) * n;
+      T dot = 0;
+      for (int i = n - 2 + lane; i < n; i += 32) {
+        const C pi = p[i], ui = up[i];
+        wp[i] = pi;
+        dot += ui.x * pi.x + ui.y * pi.y;
+      }
+      const T K = T(0.5) * tau_prev * warp_sum(dot);
+      for (int i = n - 2 + lane; i < n; i += 32) { wp[i].x -= K * up[i].x; wp[i].y -= K * up[i].y; }
+      __syncwarp();
+      if (lane < 3) {
+        const int i = (lane == 0) ? n - 2 : n - 1, j = (lane == 2) ? n - 1 : n - 2;
+        rank2(L[tri(i) + j], up[i], wp[j], wp[i], up[j]);
+      }
+      for (int i = n - 2 + lane; i < n; i += 32) L[tri(i) + n - 3] = up[i];
+      __syncwarp();
+    }
+    if (lane == 0) {
+      s.d[n - 2] = L[tri(n - 2) + n - 2].x;
+      s.d[n - 1] = L[tri(n - 1) + n - 1].x;
+      s.e[n - 2] = L[tri(n - 1) + n - 2];
+    }
+  }
+  __syncthreads();
+}
+
+
 // acc += a b
 template <typename C> __device__ __forceinline__ void cmac(C& acc, C a, C b) {
   acc.x += a.x * b.x - a.y * b.y;
@@ -322,202 +466,6 @@ template <typename C> __device__ __forceinline__ C warp_sum4(const C (&r)[4]) {
   k = cadd(k, shfl_xor_c(k, 2));
   k = cadd(k, shfl_xor_c(k, 1));
   return k;
-}
-
-// Product of the last step for row i: rowp[i] + sum of the warps' column partials.
-template <typename T>
-__device__ __forceinline__ typename C2<T>::type prod_of(const TriShared<T>& s, int n, int i) {
-  typename C2<T>::type p = s.rowp[i];
-#pragma unroll
-  for (int w = 0; w < kWarps; ++w) p = cadd(p, s.cp[w * n + i]);
-  return p;
-}
-
-// Householder reduction of the Hermitian M (lower triangle, packed in s.L) to tridiagonal
-// (s.d, s.e); reflector k is left in column k (rows k+1..n-1) with scalar s.tau[k]. The
-// whole CTA, two barriers per step k:
-//   S (warp 0): finish step k-1 (p = tau M u, K = tau/2 u^H p, w = p - K u) and form
-//     reflector k from column k with step k-1's update applied on the fly,
-//     x_i = A_i + K B_i, A_i and B_i from the same loads as the dot product;
-//   P (all warps): one pass over the trailing triangle (rows and columns k+1..n-1). Each
-//     element is loaded once: step k-1's rank-2 update is applied and stored, and the
-//     element adds to both products it takes part in, row i (M_ij u_j) and column j
-//     (conj(M_ij) u_i). A warp takes one row at a time with its lanes over the columns,
-//     rows in mirrored pairs so that every warp has the same count of elements; row sums
-//     are reduce-scattered four rows at a time, column sums stay in the lanes and are
-//     written once per warp. The S warp adds the partials in a fixed order, so results
-//     do not depend on timing.
-template <typename T>
-__device__ void tridiag_packed(const TriShared<T>& s, int n) {
-  using C = typename C2<T>::type;
-  constexpr int NC = (kMaxFastN + 31) / 32;  // column slots of a lane
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  C* L = s.L;
-  for (int k = 0; k + 2 < n; ++k) {
-    C* up = s.vec + ((k + 1) & 1) * n;  // u_{k-1}
-    C* uc = s.vec + (k & 1) * n;        // u_k
-    // ---- S: warp 0 finishes step k-1 and forms reflector k
-    if (wid == 0) {
-      const T tau_prev = k > 0 ? s.tau[k - 1] : T(0);
-      const bool pending = tau_prev != T(0);
-      C A[NC], B[NC], pp[NC], uu[NC];
-      T dot = 0;
-      C pk = mk<T>(0, 0), ukk = mk<T>(0, 0);
-      if (pending) {
-        pk = prod_of(s, n, k);
-        pk = mk<T>(tau_prev * pk.x, tau_prev * pk.y);
-        ukk = up[k];
-      }
-#pragma unroll
-      for (int t = 0; t < NC; ++t) {
-        const int i = k + lane + 32 * t;
-        A[t] = B[t] = pp[t] = uu[t] = mk<T>(0, 0);
-        if (i < n) {
-          const int base = tri(i);
-          A[t] = L[base + k];
-          if (pending) {
-            const C q = prod_of(s, n, i);
-            pp[t] = mk<T>(tau_prev * q.x, tau_prev * q.y);
-            uu[t] = up[i];
-            dot += uu[t].x * pp[t].x + uu[t].y * pp[t].y;
-            // x_i = a_ik - u_i conj(w_k) - w_i conj(u_k) = A_i + K B_i, w = p - K u
-            rank2(A[t], uu[t], pk, pp[t], ukk);
-            B[t] = mk<T>(2 * (uu[t].x * ukk.x + uu[t].y * ukk.y), 2 * (uu[t].y * ukk.x - uu[t].x * ukk.y));
-            L[base + k - 1] = uu[t];  // reflector k-1 (rows >= k) kept in column k-1
-          }
-        }
-      }
-      const T K = pending ? T(0.5) * tau_prev * warp_sum(dot) : T(0);
-      T xn2 = 0;
-#pragma unroll
-      for (int t = 0; t < NC; ++t) {
-        const int i = k + lane + 32 * t;
-        if (i < n) {
-          const C x = mk<T>(A[t].x + K * B[t].x, A[t].y + K * B[t].y);
-          if (pending) s.wp[i] = mk<T>(pp[t].x - K * uu[t].x, pp[t].y - K * uu[t].y);
-          uc[i] = x;
-          if (i >= k + 2) xn2 += x.x * x.x + x.y * x.y;
-        }
-      }
-      xn2 = warp_sum(xn2);
-      __syncwarp();
-      const C alpha = uc[k + 1];
-      T tau_k = 0;
-      C ek = alpha;
-      if (xn2 != T(0)) {
-        const T aa = sqrt(alpha.x * alpha.x + alpha.y * alpha.y);
-        const T nrm = sqrt(aa * aa + xn2);
-        const C ph1 = aa > T(0) ? mk<T>(alpha.x / aa, alpha.y / aa) : mk<T>(1, 0);
-        tau_k = T(2) / ((aa + nrm) * (aa + nrm) + xn2);
-        ek = mk<T>(-ph1.x * nrm, -ph1.y * nrm);
-        if (lane == 0) uc[k + 1] = mk<T>(ph1.x * (aa + nrm), ph1.y * (aa + nrm));
-      }
-      if (lane == 0) { s.d[k] = uc[k].x; s.e[k] = ek; s.tau[k] = tau_k; }
-    }
-    __syncthreads();
-    // ---- P: step k-1's update and the product M u_k over rows/columns k+1..n-1
-    const bool pending = k > 0 && s.tau[k - 1] != T(0);
-    const bool mv = s.tau[k] != T(0);
-    if (!pending && !mv) continue;  // CTA-uniform; nothing reads this step's product
-    const int k1 = k + 1;
-    const int m = n - k1;
-    C ui[NC], upi[NC], wpi[NC], cacc[NC];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      const int i = k1 + lane + 32 * c;
-      ui[c] = upi[c] = wpi[c] = cacc[c] = mk<T>(0, 0);
-      if (i < n) {
-        ui[c] = uc[i];
-        if (pending) { upi[c] = up[i]; wpi[c] = s.wp[i]; }
-      }
-    }
-    const int npair = (m + 1) >> 1;
-    for (int q0 = wid; q0 < npair; q0 += 2 * kWarps) {
-      // rows of this round: pair q0 and pair q0 + kWarps, each (k1 + q, n - 1 - q)
-      const bool two = q0 + kWarps < npair;
-      C racc[4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        racc[r] = mk<T>(0, 0);
-        const int q = q0 + (r >> 1) * kWarps;
-        const int jj = (r & 1) ? n - 1 - q : k1 + q;
-        if ((r >> 1) && !two) continue;         // warp-uniform
-        if ((r & 1) && jj == k1 + q) continue;  // middle row of an odd count, taken once
-        const int base = tri(jj);
-        const C ucj = uc[jj];
-        C upj = mk<T>(0, 0), wpj = mk<T>(0, 0);
-        if (pending) { upj = up[jj]; wpj = s.wp[jj]; }
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          if (k1 + 32 * c > jj) break;  // slot entirely right of the diagonal (warp-uniform)
-          const int i = k1 + lane + 32 * c;
-          if (i <= jj) {
-            C a = L[base + i];
-            if (pending) {
-              rank2(a, upj, wpi[c], wpj, upi[c]);
-              L[base + i] = a;
-            }
-            if (mv) {
-              if (i < jj) {
-                cmac(racc[r], a, ui[c]);
-                cmacc(cacc[c], a, ucj);
-              } else {
-                racc[r].x += a.x * ui[c].x;
-                racc[r].y += a.x * ui[c].y;
-              }
-            }
-          }
-        }
-      }
-      if (mv) {
-        const C tot = warp_sum4(racc);
-        const int r = lane >> 3;
-        const int q = q0 + (r >> 1) * kWarps;
-        const int jj = (r & 1) ? n - 1 - q : k1 + q;
-        const bool ok = (!(r >> 1) || two) && !((r & 1) && jj == k1 + q);
-        if ((lane & 7) == 0 && ok) s.rowp[jj] = tot;
-      }
-    }
-    if (mv) {
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        const int i = k1 + lane + 32 * c;
-        if (i < n) s.cp[wid * n + i] = cacc[c];
-      }
-    }
-    __syncthreads();
-  }
-  // last pending update (step n-3) on the trailing 2 x 2 block; reflector n-3 stored
-  if (wid == 0) {
-    if (n >= 3 && s.tau[n - 3] != T(0)) {
-      const T tau_prev = s.tau[n - 3];
-      const C* up = s.vec + ((n - 3) & 1) * n;
-      T dot = 0;
-      C pi = mk<T>(0, 0), ui = mk<T>(0, 0);
-      const int i = n - 2 + lane;
-      if (lane < 2) {
-        const C q = prod_of(s, n, i);
-        pi = mk<T>(tau_prev * q.x, tau_prev * q.y);
-        ui = up[i];
-        dot = ui.x * pi.x + ui.y * pi.y;
-      }
-      const T K = T(0.5) * tau_prev * warp_sum(dot);
-      if (lane < 2) s.wp[i] = mk<T>(pi.x - K * ui.x, pi.y - K * ui.y);
-      __syncwarp();
-      if (lane < 3) {
-        const int r = (lane == 0) ? n - 2 : n - 1, c = (lane == 2) ? n - 1 : n - 2;
-        rank2(L[tri(r) + c], up[r], s.wp[c], s.wp[r], up[c]);
-      }
-      if (lane < 2) L[tri(i) + n - 3] = up[i];
-      __syncwarp();
-    }
-    if (lane == 0) {
-      s.d[n - 2] = L[tri(n - 2) + n - 2].x;
-      s.d[n - 1] = L[tri(n - 1) + n - 1].x;
-      s.e[n - 2] = L[tri(n - 1) + n - 2];
-    }
-  }
-  __syncthreads();
 }
 
 // ----------------------------------------------------------------- workspace layout
@@ -1273,10 +1221,12 @@ __global__ void route_kernel(const uint8_t* __restrict__ sing, int64_t nb, int32
   }
 }
 
-// Column groups of the Gauss-Jordan grid: 32 (512 threads), which halves the registers a
-// thread holds and leaves room for the look-ahead column.
+// Column groups of the Gauss-Jordan grid. 32 groups (512 threads, half the registers per
+// thread) measured no faster than 16 in FP32 or FP64: one point per SM either way, and its
+// serial pivot steps set the pace. With look-ahead pivoting the 512-thread tile stayed in
+// local memory (128 registers per thread), twice as slow.
 template <typename T>
-constexpr int gj_cx() { return 32; }
+constexpr int gj_cx() { return 16; }
 
 template <typename T, int NB, typename TW>
 int launch_inverse(const float2* coh, PointSet pts, int64_t grid_cap, int n, unsigned char* ws, uint8_t* sing,
