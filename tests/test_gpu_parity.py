@@ -232,6 +232,10 @@ def test_emi_refine_vs_fp64_oracle(cuda, name, size):
     ph_r, q_r, gap, cond = O.emi(coh)
     ph, q, route = mb.emi(coh, precision="refine", return_route=True)
     ph64, q64 = mb.emi(coh, precision="fp64")
+    if cfg.nimages > 128:  # FP64 throughout above 128 images: every point reported recomputed
+        assert np.all(route == 1)
+        np.testing.assert_array_equal(ph.view(np.int32), ph64.view(np.int32))
+        return
     assert set(np.unique(route)) <= {0, 1, 2}
     kept, redone = route == 0, route == 1
     assert kept.mean() > 0.5
