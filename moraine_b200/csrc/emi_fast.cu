@@ -623,6 +623,21 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 2) reduce_kerne
   }
 }
 
+// Reflector k of a point (its scalar and the lane's four entries, zero past its end) into
+// registers.
+template <typename T, typename TA>
+__device__ __forceinline__ void load_refl(const PointPtr<T, TA>& w, int n, int k, int lane,
+                                          typename C2<T>::type (&u)[4], T& tau) {
+  tau = w.tau[k];
+  const typename C2<T>::type* src = w.refl + refl_off(k, n);
+  const int m = n - k - 1;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int i = lane + 32 * t;
+    u[t] = i < m ? src[i] : mk<T>(0, 0);
+  }
+}
+
 // ----------------------------------------------------------------- kernel 3: tail, one warp per point
 constexpr int kTailWarps = 8;
 
@@ -731,36 +746,43 @@ __global__ void __launch_bounds__(32 * kTailWarps, 3) tail_kernel(const float2* 
     // v = Q D y
     for (int i = lane; i < n; i += 32) { const C dl = z[i]; z[i] = mk<T>(dl.x * y[i], dl.y * y[i]); }
     __syncwarp();
-    for (int k = n - 3; k >= 0; --k) {
-      const T tau = w.tau[k];
-      if (tau == T(0)) continue;
-      const C* u = w.refl + refl_off(k, n);
-      const int m = n - k - 1;
-      C sacc = mk<T>(0, 0);
-      C uu[4];
+    // reflectors applied from the last; the next one's values are loaded while the current
+    // one is applied, so the serial chain does not wait on memory
+    {
+      C uu[4], nu[4];
+      T tau = 0, ntau = 0;
+      if (n >= 3) load_refl(w, n, n - 3, lane, uu, tau);
+      for (int k = n - 3; k >= 0; --k) {
+        if (k > 0) load_refl(w, n, k - 1, lane, nu, ntau);
+        if (tau != T(0)) {
+          const int m = n - k - 1;
+          C sacc = mk<T>(0, 0);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int i = lane + 32 * t;
-        uu[t] = mk<T>(0, 0);
-        if (i < m) {
-          uu[t] = u[i];
-          const C zi = z[k + 1 + i];
-          sacc.x += uu[t].x * zi.x + uu[t].y * zi.y;
-          sacc.y += uu[t].x * zi.y - uu[t].y * zi.x;
-        }
-      }
-      sacc.x = warp_sum(sacc.x);
-      sacc.y = warp_sum(sacc.y);
+          for (int t = 0; t < 4; ++t) {
+            const int i = lane + 32 * t;
+            if (i < m) {
+              const C zi = z[k + 1 + i];
+              sacc.x += uu[t].x * zi.x + uu[t].y * zi.y;
+              sacc.y += uu[t].x * zi.y - uu[t].y * zi.x;
+            }
+          }
+          sacc.x = warp_sum(sacc.x);
+          sacc.y = warp_sum(sacc.y);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int i = lane + 32 * t;
-        if (i < m) {
-          const C tt = cmul_t(uu[t], sacc);
-          z[k + 1 + i].x -= tau * tt.x;
-          z[k + 1 + i].y -= tau * tt.y;
+          for (int t = 0; t < 4; ++t) {
+            const int i = lane + 32 * t;
+            if (i < m) {
+              const C tt = cmul_t(uu[t], sacc);
+              z[k + 1 + i].x -= tau * tt.x;
+              z[k + 1 + i].y -= tau * tt.y;
+            }
+          }
+          __syncwarp();
         }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) uu[t] = nu[t];
+        tau = ntau;
       }
-      __syncwarp();
     }
     // normalise to the reference image
     const bool singular = (sing[pt] & kRouteSingular) != 0;
@@ -921,35 +943,39 @@ template <typename T, typename TA>
 __device__ void apply_q(const PointPtr<T, TA>& w, int n, double2* z, bool forward) {
   using C = typename C2<T>::type;
   const int lane = threadIdx.x & 31;
+  if (n < 3) return;
+  C cu[4], nu[4];
+  T ct = 0, nt = 0;
+  load_refl(w, n, forward ? 0 : n - 3, lane, cu, ct);
   for (int s = 0; s + 2 < n; ++s) {
     const int k = forward ? s : n - 3 - s;
-    const double tau = (double)w.tau[k];
-    if (tau == 0.0) continue;
-    const C* u = w.refl + refl_off(k, n);
-    const int m = n - k - 1;
-    double2 acc = make_double2(0, 0), uu[4];
+    if (s + 3 < n) load_refl(w, n, forward ? s + 1 : n - 4 - s, lane, nu, nt);  // the next one, early
+    const double tau = (double)ct;
+    if (tau != 0.0) {
+      const int m = n - k - 1;
+      double2 acc = make_double2(0, 0), uu[4];
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int i = lane + 32 * t;
-      uu[t] = make_double2(0, 0);
-      if (i < m) {
-        const C ui = u[i];
-        uu[t] = make_double2(ui.x, ui.y);
-        cmacc(acc, uu[t], z[k + 1 + i]);  // u^H z
+      for (int t = 0; t < 4; ++t) {
+        const int i = lane + 32 * t;
+        uu[t] = make_double2(cu[t].x, cu[t].y);
+        if (i < m) cmacc(acc, uu[t], z[k + 1 + i]);  // u^H z
       }
-    }
-    acc.x = warp_sum(acc.x);
-    acc.y = warp_sum(acc.y);
+      acc.x = warp_sum(acc.x);
+      acc.y = warp_sum(acc.y);
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int i = lane + 32 * t;
-      if (i < m) {
-        const double2 tt = cmul(uu[t], acc);
-        z[k + 1 + i].x -= tau * tt.x;
-        z[k + 1 + i].y -= tau * tt.y;
+      for (int t = 0; t < 4; ++t) {
+        const int i = lane + 32 * t;
+        if (i < m) {
+          const double2 tt = cmul(uu[t], acc);
+          z[k + 1 + i].x -= tau * tt.x;
+          z[k + 1 + i].y -= tau * tt.y;
+        }
       }
+      __syncwarp();
     }
-    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < 4; ++t) cu[t] = nu[t];
+    ct = nt;
   }
 }
 
