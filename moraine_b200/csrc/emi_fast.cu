@@ -191,7 +191,15 @@ __device__ bool gj_tile(T (&a)[NB][GjGrid<NB, CX>::NC], unsigned used, int n, in
         case 4: if (NC > 4) gj_step<T, NB, CX, (4 < NC ? 4 : 0)>(a, used, k, tx, ty, singular, s); break;
         case 5: if (NC > 5) gj_step<T, NB, CX, (5 < NC ? 5 : 0)>(a, used, k, tx, ty, singular, s); break;
         case 6: if (NC > 6) gj_step<T, NB, CX, (6 < NC ? 6 : 0)>(a, used, k, tx, ty, singular, s); break;
-        default: if (NC > 7) gj_step<T, NB, CX, (7 < NC ? 7 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 7: if (NC > 7) gj_step<T, NB, CX, (7 < NC ? 7 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 8: if (NC > 8) gj_step<T, NB, CX, (8 < NC ? 8 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 9: if (NC > 9) gj_step<T, NB, CX, (9 < NC ? 9 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 10: if (NC > 10) gj_step<T, NB, CX, (10 < NC ? 10 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 11: if (NC > 11) gj_step<T, NB, CX, (11 < NC ? 11 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 12: if (NC > 12) gj_step<T, NB, CX, (12 < NC ? 12 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 13: if (NC > 13) gj_step<T, NB, CX, (13 < NC ? 13 : 0)>(a, used, k, tx, ty, singular, s); break;
+        case 14: if (NC > 14) gj_step<T, NB, CX, (14 < NC ? 14 : 0)>(a, used, k, tx, ty, singular, s); break;
+        default: if (NC > 15) gj_step<T, NB, CX, (15 < NC ? 15 : 0)>(a, used, k, tx, ty, singular, s); break;
       }
     }
   }
