@@ -587,6 +587,164 @@ __global__ void __launch_bounds__(16 * CX, 1) inverse_kernel(const float2* __res
   }
 }
 
+// ----------------------------------------------------------------- kernel 1b: symmetric sweep
+// inv(|Gamma|) for the refined mixed precision, FP64: Gauss-Jordan on the symmetric matrix
+// with diagonal pivots in natural order (the sweep operator), which keeps the matrix
+// symmetric, so only its lower triangle is held and updated: half the registers of the
+// pivoted kernel (two CTAs per SM) and half its FMAs, with no pivot search on the serial
+// chain of a step. Step k with column c = A[:, k] (c_k = d):
+//   A_ij -= c_i c_j / d (i, j != k);  A_ik = c_i / d (i != k);  A_kk = -1 / d,
+// and after all n steps A holds -inv(A). Without interchanges a pivot can become small on
+// an indefinite |Gamma|; the kernel keeps the smallest |pivot| and flags the point
+// (kRouteCond) when it falls below kSweepMinPivot, and the refined pass recomputes flagged
+// points with the pivoted FP64 kernels. On the c2 scene model the natural order stays
+// within about 30 eps cond(|Gamma|) of the pivoted inverse (3.7e-9 relative at worst over
+// 1,500 points, 41 % of them indefinite), far below what the refinement needs.
+constexpr double kSweepMinPivot = 1e-9;
+
+template <int NB>
+struct SweepShared {
+  double col[2][16 * NB];  // column k of the step (by step parity)
+  int piv_small;
+};
+
+__host__ __device__ constexpr int lt(int ib, int jb) { return ib * (ib + 1) / 2 + jb; }  // jb <= ib
+
+// Thread (tx, ty) of the 16 x 16 grid holds A[i][j] for i = ty + 16 ib, j = tx + 16 jb,
+// jb <= ib (NB (NB + 1) / 2 values); in a diagonal block only ty >= tx is the lower triangle.
+template <int NB, int KB>
+__device__ __forceinline__ void sweep_step(double (&a)[NB * (NB + 1) / 2], int k, int n, int tx, int ty,
+                                           double& minpiv, SweepShared<NB>& s) {
+  const int buf = k & 1;
+  const double d = s.col[buf][k];
+  minpiv = fmin(minpiv, fabs(d));
+  const double rd = recip(d == 0.0 ? 1.0 : d);
+  double ci[NB], cj[NB];
+#pragma unroll
+  for (int ib = 0; ib < NB; ++ib) ci[ib] = s.col[buf][ty + 16 * ib] * rd;
+#pragma unroll
+  for (int jb = 0; jb < NB; ++jb) cj[jb] = s.col[buf][tx + 16 * jb];
+#pragma unroll
+  for (int ib = 0; ib < NB; ++ib) {
+    const int i = ty + 16 * ib;
+#pragma unroll
+    for (int jb = 0; jb <= ib; ++jb) {
+      const int j = tx + 16 * jb;
+      double& v = a[lt(ib, jb)];
+      if (i == k) v = (j == k) ? -rd : cj[jb] * rd;  // row k (j < k) and the pivot
+      else if (j == k) v = ci[ib];                  // column k (i > k)
+      else v -= ci[ib] * cj[jb];
+    }
+  }
+  // publish column k + 1 of the updated matrix: its lower part from the column-block owners,
+  // its upper part (row k + 1, by symmetry) from the row-block owners
+  const int k1 = k + 1;
+  if (k1 < n) {
+    const int kb1 = k1 >> 4, kt1 = k1 & 15;
+    double* out = s.col[buf ^ 1];
+    if (kb1 == KB) {
+      if (tx == kt1) {
+#pragma unroll
+        for (int ib = KB; ib < NB; ++ib) {
+          const int i = ty + 16 * ib;
+          if (i >= k1) out[i] = a[lt(ib, KB)];
+        }
+      }
+      if (ty == kt1) {
+#pragma unroll
+        for (int jb = 0; jb <= KB; ++jb) {
+          const int j = tx + 16 * jb;
+          if (j < k1) out[j] = a[lt(KB, jb)];
+        }
+      }
+    } else if (KB + 1 < NB) {
+      constexpr int K1 = KB + 1 < NB ? KB + 1 : 0;
+      if (tx == kt1) {
+#pragma unroll
+        for (int ib = K1; ib < NB; ++ib) {
+          const int i = ty + 16 * ib;
+          if (i >= k1) out[i] = a[lt(ib, K1)];
+        }
+      }
+      if (ty == kt1) {
+#pragma unroll
+        for (int jb = 0; jb <= K1; ++jb) {
+          const int j = tx + 16 * jb;
+          if (j < k1) out[j] = a[lt(K1, jb)];
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// TW: arithmetic of the reduction that reads the workspace (the point stride depends on it).
+template <int NB, typename TW>
+__global__ void __launch_bounds__(256, 2) sweep_kernel(const float2* __restrict__ coh, PointSet pts, int n,
+                                                       unsigned char* __restrict__ ws, uint8_t* __restrict__ sing) {
+  constexpr int NP = NB * (NB + 1) / 2;
+  __shared__ SweepShared<NB> ss;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int64_t npairs = (int64_t)n * (n - 1) / 2;
+  const int64_t npt = pts.size();
+  for (int64_t pt = blockIdx.x; pt < npt; pt += gridDim.x) {
+    const float2* c = coh + pts[pt] * npairs;
+    double a[NP];
+    // |Gamma| (identity on the padding), lower triangle
+#pragma unroll
+    for (int ib = 0; ib < NB; ++ib) {
+      const int i = ty + 16 * ib;
+#pragma unroll
+      for (int jb = 0; jb <= ib; ++jb) {
+        const int j = tx + 16 * jb;
+        double v = (i == j) ? 1.0 : 0.0;
+        if (i < n && j < n && i > j) {
+          const float2 g = c[triu_index(j, i, n)];
+          v = sqrt((double)g.x * g.x + (double)g.y * g.y);
+        }
+        a[lt(ib, jb)] = v;
+      }
+    }
+    // column 0: the lower part from column-block 0, no upper part
+    if (tx == 0) {
+#pragma unroll
+      for (int ib = 0; ib < NB; ++ib) ss.col[0][ty + 16 * ib] = a[lt(ib, 0)];
+    }
+    __syncthreads();
+    double minpiv = 1e300;
+#pragma unroll 1
+    for (int kb = 0; kb < NB; ++kb) {
+      for (int kt = 0; kt < 16; ++kt) {
+        const int k = 16 * kb + kt;
+        if (k >= n) break;
+        switch (kb) {  // compile-time block for each kb
+          case 0: sweep_step<NB, 0>(a, k, n, tx, ty, minpiv, ss); break;
+          case 1: if (NB > 1) sweep_step<NB, (1 < NB ? 1 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
+          case 2: if (NB > 2) sweep_step<NB, (2 < NB ? 2 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
+          case 3: if (NB > 3) sweep_step<NB, (3 < NB ? 3 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
+          case 4: if (NB > 4) sweep_step<NB, (4 < NB ? 4 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
+          case 5: if (NB > 5) sweep_step<NB, (5 < NB ? 5 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
+          case 6: if (NB > 6) sweep_step<NB, (6 < NB ? 6 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
+          default: if (NB > 7) sweep_step<NB, (7 < NB ? 7 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
+        }
+      }
+    }
+    // every thread saw the same pivots: minpiv is uniform
+    double* out = PointPtr<TW, double>(ws, pt, n).ainv;
+#pragma unroll
+    for (int ib = 0; ib < NB; ++ib) {
+      const int i = ty + 16 * ib;
+#pragma unroll
+      for (int jb = 0; jb <= ib; ++jb) {
+        const int j = tx + 16 * jb;
+        if (i < n && j <= i) out[tri_up(j, i, n)] = -a[lt(ib, jb)];  // inv = -A after the sweep
+      }
+    }
+    if (tid == 0) sing[pt] = (minpiv < kSweepMinPivot || !(minpiv == minpiv)) ? kRouteCond : 0;
+    __syncthreads();
+  }
+}
+
 // ----------------------------------------------------------------- kernel 2: reduction
 template <typename T, typename TA>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 2) reduce_kernel(const float2* __restrict__ coh, PointSet pts, int n,
@@ -1167,7 +1325,8 @@ __global__ void __launch_bounds__(32 * kRefineWarps) tail_refine_kernel(
     const double gap = (double)lam2 - lam - 4.0 * (double)eps * (double)n * (double)tnorm;
     const double bound = rn / (gap * vmin);
     const bool singular = (sing[pt] & kRouteSingular) != 0;
-    const bool ok = singular || (gap > 0.0 && bound <= tol);
+    const bool small_pivot = (sing[pt] & kRouteCond) != 0;  // the sweep's inverse is not trusted
+    const bool ok = singular || (!small_pivot && gap > 0.0 && bound <= tol);
     // normalise to the reference image
     const double2 zr = v[ref];
     for (int i = lane; i < n; i += 32) {
@@ -1318,11 +1477,33 @@ int run_pass(const float2* c, PointSet pts, int n, int ref, float2* ph, float* q
   return check_launch("emi tail");
 }
 
-// The refined pass: FP64 inverse, FP32 reduction, FP64-refined tail; sing[] ends with the
-// points whose refined error bound exceeds `tol` flagged kRouteCond.
+template <int NB>
+int launch_sweep(const float2* c, PointSet pts, int n, unsigned char* ws, uint8_t* sing, cudaStream_t s) {
+  const int occ = std::max(1, occupancy(sweep_kernel<NB, float>, 256, 0));
+  const int64_t grid = std::min<int64_t>(pts.n_pc, (int64_t)sm_count() * occ);
+  KernelTimer kt(pts.list ? "emi sweep rerun" : "emi sweep fp64", s);
+  sweep_kernel<NB, float><<<(unsigned)grid, 256, 0, s>>>(c, pts, n, ws, sing);
+  return check_launch("emi sweep");
+}
+
+int run_sweep(const float2* c, PointSet pts, int n, unsigned char* ws, uint8_t* sing, cudaStream_t s) {
+  switch ((n + 15) / 16) {
+    case 1: case 2: return launch_sweep<2>(c, pts, n, ws, sing, s);
+    case 3: return launch_sweep<3>(c, pts, n, ws, sing, s);
+    case 4: return launch_sweep<4>(c, pts, n, ws, sing, s);
+    case 5: return launch_sweep<5>(c, pts, n, ws, sing, s);
+    case 6: return launch_sweep<6>(c, pts, n, ws, sing, s);
+    case 7: return launch_sweep<7>(c, pts, n, ws, sing, s);
+    default: return launch_sweep<8>(c, pts, n, ws, sing, s);
+  }
+}
+
+// The refined pass: FP64 inverse (symmetric sweep), FP32 reduction, FP64-refined tail;
+// sing[] ends with the points whose sweep met a small pivot or whose refined error bound
+// exceeds `tol` flagged kRouteCond.
 int run_refine_pass(const float2* c, PointSet pts, int n, int ref, float2* ph, float* quality, float* tcoh,
                     unsigned char* ws, uint8_t* sing, double tol, cudaStream_t s) {
-  if (int rc = run_inverse<double, float>(c, pts, n, ws, sing, 0.f, s)) return rc;
+  if (int rc = run_sweep(c, pts, n, ws, sing, s)) return rc;
   if (int rc = run_reduce<float, double>(c, pts, n, ws, s)) return rc;
   const size_t tsmem = kRefineWarps * refine_warp_bytes(n);
   if (int rc_ = allow_smem(reinterpret_cast<const void*>(tail_refine_kernel<float>), tsmem)) return rc_;
