@@ -629,8 +629,12 @@ __device__ __forceinline__ void sweep_step(double (&a)[NB * (NB + 1) / 2], int k
     const int i = ty + 16 * ib;
 #pragma unroll
     for (int jb = 0; jb <= ib; ++jb) {
-      const int j = tx + 16 * jb;
       double& v = a[lt(ib, jb)];
+      if (ib != KB && jb != KB) {  // compile-time: k is in neither this row nor this column block
+        v -= ci[ib] * cj[jb];
+        continue;
+      }
+      const int j = tx + 16 * jb;
       if (i == k) v = (j == k) ? -rd : cj[jb] * rd;  // row k (j < k) and the pivot
       else if (j == k) v = ci[ib];                  // column k (i > k)
       else v -= ci[ib] * cj[jb];
@@ -1167,7 +1171,7 @@ __device__ T multisect(const T* d, const T* b2, int n, T lo, T hi, int target, T
 }
 
 template <typename T>
-__global__ void __launch_bounds__(32 * kRefineWarps) tail_refine_kernel(
+__global__ void __launch_bounds__(32 * kRefineWarps, 4) tail_refine_kernel(
     const float2* __restrict__ coh, PointSet pts, int n, int ref, const unsigned char* __restrict__ ws,
     uint8_t* __restrict__ sing, float2* __restrict__ ph, float* __restrict__ quality, float* __restrict__ tcoh,
     double tol) {
