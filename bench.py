@@ -243,7 +243,7 @@ def kernel_rooflines(cfg, ktimes: dict, n_ds: int, res, peaks: dict, fp32: float
       ks merge          pixel: 4N + W + 4 bytes (keys in, mask and count out)     HBM (as asked;
                         its real limit is integer issue: W(2N-1) merge steps per pixel)
       gram fp32/fp64    DS point: 8 S Q + 3 S N flops (S its SHP count)          FP32 / FP64 pipe
-      emi inverse       DS point: N^3/3 + N^3 flops (factorisation and inverse of |Gamma|)
+      emi inverse/sweep DS point: N^3/3 + N^3 flops (factorisation and inverse of |Gamma|)
       emi reduce        DS point: 4N^3/3 flops (the complex factorisation of M)
       emi tail          DS point: 80 N^2 flops (solves, back-transformation)
     The EMI split follows the terms of the stage's 2.7 N^3 + 80 N^2 figure; the kernels
@@ -283,13 +283,16 @@ def kernel_rooflines(cfg, ktimes: dict, n_ds: int, res, peaks: dict, fp32: float
                        + (", halved for the FP64 pipe" if name.endswith("fp64") else ""))
         elif name.startswith("emi") and n_ds and "rerun" not in name:
             pts = n_ds / launches
-            if "inverse" in name:
+            if "inverse" in name:  # pivoted Gauss-Jordan
                 alg, exe = 4 * n ** 3 / 3, 2 * n ** 3
+            elif "sweep" in name:  # symmetric sweep: the lower triangle only
+                alg, exe = 4 * n ** 3 / 3, n ** 3
             elif "reduce" in name:
                 alg, exe = 4 * n ** 3 / 3, 16 * n ** 3 / 3
             else:
                 alg, exe = 80 * n ** 2, None
-            f64 = name.endswith("fp64")
+            # the refined tail's flops are its FP64 residuals and correction
+            f64 = name.endswith("fp64") or "refine" in name
             peak = fp32 / 2 if f64 else fp32
             ent.update(bound="fp64-simt" if f64 else "fp32-simt", unit="TFLOP/s",
                        achieved=alg * pts / (per / 1e3) / 1e12, peak=peak,

@@ -250,6 +250,13 @@ int mr_gamma_decode(const void* be, int64_t n, int dtype, void* out, int64_t out
  * singular at the arithmetic used get NaN (the reference's inv raises on them).
  * workspace: >= mr_emi_workspace_bytes() (the same for every precision). */
 size_t mr_emi_workspace_bytes(int64_t n_pc, int nimages);
+
+/* EMI for N <= 128 runs in sub-batches of points (per-point state in the workspace, at most
+ * 4 GiB of it by default: about 34,600 points at N = 100). mr_set_emi_sub_batch(m) caps a
+ * sub-batch at m points (0 restores the default; negative: MR_ERR_INVALID), which lowers
+ * mr_emi_workspace_bytes for later calls; a workspace sized before a larger cap was set is
+ * rejected (MR_ERR_WORKSPACE). Process-wide. No reference counterpart. */
+int mr_set_emi_sub_batch(int64_t max_points);
 int mr_emi(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, int precision,
            mr_complex64* ph, float* emi_quality, float* t_coh, void* workspace,
            size_t workspace_bytes, mr_stream_t stream);

@@ -33,6 +33,7 @@ _SIGNATURES = {
     "mr_kernel_timing": (c_int, [c_int, P, P, P]),
     "mr_gamma_sample_bytes": (c_size_t, [c_int]),
     "mr_set_autotune": (None, [c_int]),
+    "mr_set_emi_sub_batch": (c_int, [c_int64]),
     "mr_ks_plan": (c_int, [c_int, c_int, c_int, P, P, P]),
     "mr_ds_chain_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_int, c_int, c_int64]),
     "mr_ds_chain": (c_int, [P, c_int, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_int, c_int, P, P, P, P,

@@ -24,6 +24,7 @@
 // the kernel below (FP64 throughout), whose N x N working matrices live in a per-CTA
 // slice of a global workspace.
 #include <algorithm>
+#include <atomic>
 
 #include "emi_common.cuh"
 
@@ -31,6 +32,7 @@ namespace mr {
 namespace emi {
 
 // emi_fast.cu
+extern std::atomic<int64_t> g_sub_batch_cap;
 int fast_supported(int n);
 size_t fast_workspace_bytes(int64_t n_pc, int n);
 int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, float cond_max, float2* ph,
@@ -220,6 +222,12 @@ size_t general_workspace_bytes(int64_t n_pc, int n) {
 
 using namespace mr;
 using namespace mr::emi;
+
+extern "C" int mr_set_emi_sub_batch(int64_t max_points) {
+  if (max_points < 0) return fail(MR_ERR_INVALID, "set_emi_sub_batch: max_points %lld < 0", (long long)max_points);
+  mr::emi::g_sub_batch_cap.store(max_points);
+  return MR_OK;
+}
 
 extern "C" size_t mr_emi_workspace_bytes(int64_t n_pc, int nimages) {
   if (n_pc <= 0 || nimages <= 0) return 16;

@@ -20,11 +20,16 @@
 // tail of many points overlaps on one SM, and the register-bound inverse is not held
 // back by the shared memory of the reduction.
 #include <algorithm>
+#include <atomic>
 
 #include "emi_common.cuh"
 
 namespace mr {
 namespace emi {
+
+// Largest sub-batch a caller asked for (mr_set_emi_sub_batch); 0: the default.
+std::atomic<int64_t> g_sub_batch_cap{0};
+
 namespace {
 
 constexpr int kMaxFastN = 128;
@@ -274,8 +279,9 @@ __device__ inline TriShared<T> tri_layout(unsigned char* base, int n) {
 
 // a -= ui conj(wj) + wi conj(uj)
 template <typename C> __device__ __forceinline__ void rank2(C& a, C ui, C wj, C wi, C uj) {
-  a.x -= ui.x * wj.x + ui.y * wj.y + wi.x * uj.x + wi.y * uj.y;
-  a.y -= ui.y * wj.x - ui.x * wj.y + wi.y * uj.x - wi.x * uj.y;
+  // one FMA per product (no separate multiply and add)
+  a.x -= ui.x * wj.x; a.x -= ui.y * wj.y; a.x -= wi.x * uj.x; a.x -= wi.y * uj.y;
+  a.y -= ui.y * wj.x; a.y += ui.x * wj.y; a.y -= wi.y * uj.x; a.y += wi.x * uj.y;
 }
 
 // Householder reduction of the Hermitian M (lower triangle, packed in s.L) to tridiagonal
@@ -287,9 +293,8 @@ template <typename C> __device__ __forceinline__ void rank2(C& a, C ui, C wj, C 
 //   2. phase 1: step k-1's rank-2 update on the lower triangle of rows >= k+1 and the row
 //      part of (M u_k)_i = sum_{j<=i} M_ij u_j;
 //   3. phase 2: the column part sum_{j>i} conj(M_ji) u_j, then p_k = tau_k M u_k.
-// Rows are handled in mirrored pairs (i, n+k-i) by groups of 4 to 32 threads (as many as
-// keep the CTA busy while the trailing matrix shrinks), which gives every thread of a step
-// the same number of elements in both phases. The packed triangle halves the
+// Rows are handled in mirrored pairs (i, n+k-i) by groups of 4 threads, which gives every
+// thread of a step the same number of elements in both phases. The packed triangle halves the
 // shared memory of full storage, so twice as many points are in flight per SM.
 template <typename T>
 __device__ void tridiag_packed(const TriShared<T>& s, int n) {
@@ -359,9 +364,10 @@ __device__ void tridiag_packed(const TriShared<T>& s, int n) {
     const T tau_k = s.tau[k];
     const int m = n - k - 1;         // rows k+1..n-1
     const int npair = (m + 1) >> 1;  // mirrored pairs (the middle row of an odd m alone)
-    // G threads per pair, as many as keep every thread of the CTA busy (4 to 32)
-    int G = 4;
-    while (G < 32 && npair * G * 2 <= (int)blockDim.x) G <<= 1;
+    // G = 4 threads per pair. Widening the groups to keep every thread busy as the trailing
+    // matrix shrinks measured 3 % slower: the short rows of late steps then cost more loop
+    // set-up than they save, while idle warps leave the issue slots to the other CTAs.
+    const int G = 4;
     const int pq = tid / G, sub = tid & (G - 1);
     const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u) << (lane & ~(G - 1));
     const bool active = (pending || tau_k != T(0)) && pq < npair;
@@ -382,8 +388,8 @@ __device__ void tridiag_packed(const TriShared<T>& s, int n) {
           C a = row[j];
           if (pending) { rank2(a, upi, wp[j], wpi, up[j]); row[j] = a; }
           const C u = uc[j];
-          acc.x += a.x * u.x - a.y * u.y;
-          acc.y += a.x * u.y + a.y * u.x;
+          acc.x += a.x * u.x; acc.x -= a.y * u.y;
+          acc.y += a.x * u.y; acc.y += a.y * u.x;
         }
         if (r) rs2 = acc; else rs1 = acc;
       }
@@ -399,8 +405,8 @@ __device__ void tridiag_packed(const TriShared<T>& s, int n) {
         for (int j = i + 1 + sub; j < n; j += G) {
           const C a = L[tri(j) + i];  // M_ji, lower triangle
           const C u = uc[j];
-          acc.x += a.x * u.x + a.y * u.y;  // conj(M_ji) u_j
-          acc.y += a.x * u.y - a.y * u.x;
+          acc.x += a.x * u.x; acc.x += a.y * u.y;  // conj(M_ji) u_j
+          acc.y += a.x * u.y; acc.y -= a.y * u.x;
         }
         for (int o = 1; o < G; o <<= 1) {
           acc.x += __shfl_xor_sync(gmask, acc.x, o);
@@ -526,7 +532,8 @@ __host__ __device__ __forceinline__ size_t refl_off(int k, int n) { return (size
 constexpr uint8_t kRouteCond = 1;      // cond_1(|Gamma|) estimate above the threshold
 constexpr uint8_t kRouteSingular = 2;  // a zero pivot: |Gamma| singular at this precision
 
-// Points of a pass: all n_pc of the sub-batch, or list[0 .. *count) of them.
+// Points of a pass: all n_pc of the sub-batch; or, with a list, list[off + i] for
+// i < min(*count - off, n_pc), a window of at most n_pc entries of a list that may be longer.
 struct PointSet {
   const int32_t* list;
   const int32_t* count;
@@ -534,14 +541,13 @@ struct PointSet {
   const int64_t* dcount;  // without a list: the points are dcount[0] - off, at most n_pc
   int64_t off;
   __device__ __forceinline__ int64_t size() const {
-    if (list) return (int64_t)*count;
-    if (dcount) {
-      const int64_t c = *dcount - off;
+    if (list || dcount) {
+      const int64_t c = (list ? (int64_t)*count : *dcount) - off;
       return c < 0 ? 0 : (c < n_pc ? c : n_pc);
     }
     return n_pc;
   }
-  __device__ __forceinline__ int64_t operator[](int64_t i) const { return list ? (int64_t)list[i] : i; }
+  __device__ __forceinline__ int64_t operator[](int64_t i) const { return list ? (int64_t)list[off + i] : i; }
 };
 
 // TW: arithmetic of the reduction that reads the workspace (the point stride depends on it).
@@ -595,8 +601,8 @@ __global__ void __launch_bounds__(16 * CX, 1) inverse_kernel(const float2* __res
 // chain of a step. Step k with column c = A[:, k] (c_k = d):
 //   A_ij -= c_i c_j / d (i, j != k);  A_ik = c_i / d (i != k);  A_kk = -1 / d,
 // and after all n steps A holds -inv(A). Without interchanges a pivot can become small on
-// an indefinite |Gamma|; the kernel keeps the smallest |pivot| and flags the point
-// (kRouteCond) when it falls below kSweepMinPivot, and the refined pass recomputes flagged
+// an indefinite |Gamma|; the kernel flags the point (kRouteCond) when a pivot falls below
+// kSweepMinPivot in magnitude, and the refined pass recomputes flagged
 // points with the pivoted FP64 kernels. On the c2 scene model the natural order stays
 // within about 30 eps cond(|Gamma|) of the pivoted inverse (3.7e-9 relative at worst over
 // 1,500 points, 41 % of them indefinite), far below what the refinement needs.
@@ -604,80 +610,102 @@ constexpr double kSweepMinPivot = 1e-9;
 
 template <int NB>
 struct SweepShared {
-  double col[2][16 * NB];  // column k of the step (by step parity)
-  int piv_small;
+  double2 col[2][16 * NB];  // columns k and k + 1 of a pivot pair, (A_ik, A_i,k+1), by pair parity
 };
 
 __host__ __device__ constexpr int lt(int ib, int jb) { return ib * (ib + 1) / 2 + jb; }  // jb <= ib
 
 // Thread (tx, ty) of the 16 x 16 grid holds A[i][j] for i = ty + 16 ib, j = tx + 16 jb,
-// jb <= ib (NB (NB + 1) / 2 values); in a diagonal block only ty >= tx is the lower triangle.
+// jb <= ib (NB (NB + 1) / 2 values); in a diagonal block only ty >= tx is the lower triangle
+// (the rest is updated like it but never read).
+//
+// Pivots go in pairs K = {k, k + 1} (k even; with n odd the last pair takes the identity row
+// of the padding): with P = A_KK, the two sweeps at once are
+//   A_ij -= A_iK inv(P) A_Kj (i, j not in K);  A_iK = A_iK inv(P);  A_KK = -inv(P),
+// one barrier per pair, evaluated as the two single sweeps in sequence (sweep_pair). The
+// owners of columns k, k + 1 (two lanes of every half-warp) write A_iK, the owners of rows
+// k, k + 1 (one whole warp, as ty = k, k + 1 share a warp) write A_Kj and -inv(P). The
+// point is flagged when a natural-order pivot (P_00, then P_11 - P_10^2 / P_00) falls below
+// kSweepMinPivot.
+
+// Columns k2, k2 + 1 of the matrix into `out`: the lower parts (rows >= k2, >= k2 + 1) from
+// the owners of those columns, the upper parts from the owners of rows k2, k2 + 1 (symmetry).
+// KBX = k2 >> 4 at compile time.
+template <int NB, int KBX>
+__device__ __forceinline__ void sweep_publish(const double (&a)[NB * (NB + 1) / 2], int k2, int tx, int ty,
+                                              double2* out) {
+  const int kt2 = k2 & 15;
+  if (tx == kt2 || tx == kt2 + 1) {
+    const int c = tx - kt2;
+#pragma unroll
+    for (int ib = KBX; ib < NB; ++ib) {
+      const int i = ty + 16 * ib;
+      if (i >= k2 + c) (c ? out[i].y : out[i].x) = a[lt(ib, KBX)];
+    }
+  }
+  if (ty == kt2 || ty == kt2 + 1) {
+    const int r = ty - kt2;
+#pragma unroll
+    for (int jb = 0; jb <= KBX; ++jb) {
+      const int j = tx + 16 * jb;
+      if (j < k2 + r) (r ? out[j].y : out[j].x) = a[lt(KBX, jb)];
+    }
+  }
+}
+
 template <int NB, int KB>
-__device__ __forceinline__ void sweep_step(double (&a)[NB * (NB + 1) / 2], int k, int n, int tx, int ty,
-                                           double& minpiv, SweepShared<NB>& s) {
-  const int buf = k & 1;
-  const double d = s.col[buf][k];
-  minpiv = fmin(minpiv, fabs(d));
-  const double rd = recip(d == 0.0 ? 1.0 : d);
-  double ci[NB], cj[NB];
+__device__ __forceinline__ void sweep_pair(double (&a)[NB * (NB + 1) / 2], int k, int n, int tx, int ty,
+                                           bool& small, SweepShared<NB>& s) {
+  const int buf = (k >> 1) & 1;
+  const double2* col = s.col[buf];
+  const int kt = k & 15;
+  const double2 pk = col[k], pk1 = col[k + 1];
+  // the two sweeps in sequence, fused: sweep k turns column k + 1 into c1' = c1 - t c0
+  // (t = P_10 / P_00) and its pivot into d1 = P_11 - t P_10; then
+  //   A_ij -= g0_i c0_j + g1_i c1'_j,  g0 = c0 / P_00, g1 = c1' / d1,
+  // the same two roundings per element as two single sweeps (the product form
+  // c_i inv(P) c_j^T instead loses accuracy to cancellation when d1 is small)
+  const double r0 = recip(pk.x == 0.0 ? 1.0 : pk.x);
+  const double t = pk.y * r0;
+  const double d1 = pk1.y - t * pk.y;
+  const double r1 = recip(d1 == 0.0 ? 1.0 : d1);
+  // natural-order pivots P_00 and d1; NaN compares false and is flagged too
+  small |= !(fabs(pk.x) >= kSweepMinPivot && fabs(d1) >= kSweepMinPivot);
+  double2 cj[NB];  // (c0_j, c1'_j)
 #pragma unroll
-  for (int ib = 0; ib < NB; ++ib) ci[ib] = s.col[buf][ty + 16 * ib] * rd;
-#pragma unroll
-  for (int jb = 0; jb < NB; ++jb) cj[jb] = s.col[buf][tx + 16 * jb];
+  for (int jb = 0; jb < NB; ++jb) {
+    const double2 c = col[tx + 16 * jb];
+    cj[jb] = make_double2(c.x, c.y - t * c.x);
+  }
+  const bool colk = tx == kt || tx == kt + 1;  // this lane owns column k or k + 1 (block KB)
 #pragma unroll
   for (int ib = 0; ib < NB; ++ib) {
-    const int i = ty + 16 * ib;
+    const double2 ci = col[ty + 16 * ib];
+    const double g0 = ci.x * r0, g1 = (ci.y - t * ci.x) * r1;
 #pragma unroll
     for (int jb = 0; jb <= ib; ++jb) {
       double& v = a[lt(ib, jb)];
-      if (ib != KB && jb != KB) {  // compile-time: k is in neither this row nor this column block
-        v -= ci[ib] * cj[jb];
-        continue;
-      }
-      const int j = tx + 16 * jb;
-      if (i == k) v = (j == k) ? -rd : cj[jb] * rd;  // row k (j < k) and the pivot
-      else if (j == k) v = ci[ib];                  // column k (i > k)
-      else v -= ci[ib] * cj[jb];
+      v -= g0 * cj[jb].x;
+      v -= g1 * cj[jb].y;
+      if (jb == KB && colk) v = tx == kt ? g0 - t * g1 : g1;  // A_iK = c_i inv(P)
     }
   }
-  // publish column k + 1 of the updated matrix: its lower part from the column-block owners,
-  // its upper part (row k + 1, by symmetry) from the row-block owners
-  const int k1 = k + 1;
-  if (k1 < n) {
-    const int kb1 = k1 >> 4, kt1 = k1 & 15;
-    double* out = s.col[buf ^ 1];
-    if (kb1 == KB) {
-      if (tx == kt1) {
+  if (ty == kt || ty == kt + 1) {  // rows k, k + 1: warp-uniform
+    const bool row1 = ty != kt;
 #pragma unroll
-        for (int ib = KB; ib < NB; ++ib) {
-          const int i = ty + 16 * ib;
-          if (i >= k1) out[i] = a[lt(ib, KB)];
-        }
-      }
-      if (ty == kt1) {
-#pragma unroll
-        for (int jb = 0; jb <= KB; ++jb) {
-          const int j = tx + 16 * jb;
-          if (j < k1) out[j] = a[lt(KB, jb)];
-        }
-      }
-    } else if (KB + 1 < NB) {
-      constexpr int K1 = KB + 1 < NB ? KB + 1 : 0;
-      if (tx == kt1) {
-#pragma unroll
-        for (int ib = K1; ib < NB; ++ib) {
-          const int i = ty + 16 * ib;
-          if (i >= k1) out[i] = a[lt(ib, K1)];
-        }
-      }
-      if (ty == kt1) {
-#pragma unroll
-        for (int jb = 0; jb <= K1; ++jb) {
-          const int j = tx + 16 * jb;
-          if (j < k1) out[j] = a[lt(K1, jb)];
-        }
-      }
+    for (int jb = 0; jb <= KB; ++jb) {
+      const double g0 = cj[jb].x * r0, g1 = cj[jb].y * r1;
+      double w = row1 ? g1 : g0 - t * g1;  // A_Kj = inv(P) c_j^T
+      if (jb == KB && colk)                // -inv(P)
+        w = row1 ? (tx == kt ? t * r1 : -r1) : (tx == kt ? -(r0 + t * t * r1) : t * r1);
+      a[lt(KB, jb)] = w;
     }
+  }
+  const int k2 = k + 2;
+  if (k2 < n) {
+    double2* out = s.col[buf ^ 1];
+    if (kt + 2 < 16) sweep_publish<NB, KB>(a, k2, tx, ty, out);
+    else if (KB + 1 < NB) sweep_publish<NB, (KB + 1 < NB ? KB + 1 : 0)>(a, k2, tx, ty, out);
   }
   __syncthreads();
 }
@@ -709,31 +737,27 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(const float2* __restrict_
         a[lt(ib, jb)] = v;
       }
     }
-    // column 0: the lower part from column-block 0, no upper part
-    if (tx == 0) {
-#pragma unroll
-      for (int ib = 0; ib < NB; ++ib) ss.col[0][ty + 16 * ib] = a[lt(ib, 0)];
-    }
+    sweep_publish<NB, 0>(a, 0, tx, ty, ss.col[0]);
     __syncthreads();
-    double minpiv = 1e300;
+    bool small = false;
 #pragma unroll 1
     for (int kb = 0; kb < NB; ++kb) {
-      for (int kt = 0; kt < 16; ++kt) {
+      for (int kt = 0; kt < 16; kt += 2) {
         const int k = 16 * kb + kt;
         if (k >= n) break;
         switch (kb) {  // compile-time block for each kb
-          case 0: sweep_step<NB, 0>(a, k, n, tx, ty, minpiv, ss); break;
-          case 1: if (NB > 1) sweep_step<NB, (1 < NB ? 1 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
-          case 2: if (NB > 2) sweep_step<NB, (2 < NB ? 2 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
-          case 3: if (NB > 3) sweep_step<NB, (3 < NB ? 3 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
-          case 4: if (NB > 4) sweep_step<NB, (4 < NB ? 4 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
-          case 5: if (NB > 5) sweep_step<NB, (5 < NB ? 5 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
-          case 6: if (NB > 6) sweep_step<NB, (6 < NB ? 6 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
-          default: if (NB > 7) sweep_step<NB, (7 < NB ? 7 : 0)>(a, k, n, tx, ty, minpiv, ss); break;
+          case 0: sweep_pair<NB, 0>(a, k, n, tx, ty, small, ss); break;
+          case 1: if (NB > 1) sweep_pair<NB, (1 < NB ? 1 : 0)>(a, k, n, tx, ty, small, ss); break;
+          case 2: if (NB > 2) sweep_pair<NB, (2 < NB ? 2 : 0)>(a, k, n, tx, ty, small, ss); break;
+          case 3: if (NB > 3) sweep_pair<NB, (3 < NB ? 3 : 0)>(a, k, n, tx, ty, small, ss); break;
+          case 4: if (NB > 4) sweep_pair<NB, (4 < NB ? 4 : 0)>(a, k, n, tx, ty, small, ss); break;
+          case 5: if (NB > 5) sweep_pair<NB, (5 < NB ? 5 : 0)>(a, k, n, tx, ty, small, ss); break;
+          case 6: if (NB > 6) sweep_pair<NB, (6 < NB ? 6 : 0)>(a, k, n, tx, ty, small, ss); break;
+          default: if (NB > 7) sweep_pair<NB, (7 < NB ? 7 : 0)>(a, k, n, tx, ty, small, ss); break;
         }
       }
     }
-    // every thread saw the same pivots: minpiv is uniform
+    // every thread saw the same pivots: `small` is uniform
     double* out = PointPtr<TW, double>(ws, pt, n).ainv;
 #pragma unroll
     for (int ib = 0; ib < NB; ++ib) {
@@ -744,7 +768,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(const float2* __restrict_
         if (i < n && j <= i) out[tri_up(j, i, n)] = -a[lt(ib, jb)];  // inv = -A after the sweep
       }
     }
-    if (tid == 0) sing[pt] = (minpiv < kSweepMinPivot || !(minpiv == minpiv)) ? kRouteCond : 0;
+    if (tid == 0) sing[pt] = small ? kRouteCond : 0;
     __syncthreads();
   }
 }
@@ -1008,50 +1032,69 @@ __host__ __device__ inline size_t refine_warp_bytes(int n) {
          3 * align16((size_t)n * sizeof(double2));
 }
 
-// Solve (R - lambda I) x = y in place for a complex y, R real symmetric tridiagonal (d, b):
-// the elimination of tridiag_solve with the right-hand side carried as two real columns.
-__device__ inline void tridiag_solve_c(const double* d, const double* b, int n, double lambda, double tiny,
-                                       double2* y, double* dd, double* du, double* dl) {
+// Solve (R - lambda I) x = y in place, R real symmetric tridiagonal (d, b), by elimination
+// with row interchanges, for a real (V = T) or complex (V = C2<T>) right-hand side. Each
+// row's final pivot is inverted once and kept in dd, so the back substitution multiplies:
+// one reciprocal per row on the serial chain instead of a division per row and component.
+// dd, du, dl: work arrays of length n; dl ends as the second super-diagonal of each row.
+template <typename T> __device__ __forceinline__ void axpy_r(T& y, T f, const T& x) { y -= f * x; }
+template <typename T> __device__ __forceinline__ void axpy_r(typename C2<T>::type& y, T f,
+                                                              const typename C2<T>::type& x) {
+  y.x -= f * x.x;
+  y.y -= f * x.y;
+}
+template <typename T> __device__ __forceinline__ void scale_r(T& y, T f) { y *= f; }
+template <typename T> __device__ __forceinline__ void scale_r(typename C2<T>::type& y, T f) {
+  y.x *= f;
+  y.y *= f;
+}
+
+template <typename T, typename V>
+__device__ inline void tridiag_solve_rcp(const T* d, const T* b, int n, T lambda, T tiny, V* y, T* dd, T* du,
+                                         T* dl) {
   for (int i = 0; i < n; ++i) {
     dd[i] = d[i] - lambda;
     if (i < n - 1) { du[i] = b[i]; dl[i] = b[i]; }
   }
   for (int i = 0; i < n - 1; ++i) {
-    const double sub = dl[i];
+    const T sub = dl[i];
     if (fabs(dd[i]) >= fabs(sub)) {
-      if (dd[i] == 0.0) dd[i] = tiny;
-      const double f = sub / dd[i];
+      if (dd[i] == T(0)) dd[i] = tiny;
+      const T r = recip(dd[i]);
+      const T f = sub * r;
       dd[i + 1] -= f * du[i];
-      y[i + 1].x -= f * y[i].x;
-      y[i + 1].y -= f * y[i].y;
-      dl[i] = 0.0;
+      axpy_r<T>(y[i + 1], f, y[i]);
+      dl[i] = T(0);
+      dd[i] = r;
     } else {
-      const double f = dd[i] / sub;
-      dd[i] = sub;
-      const double t = dd[i + 1];
+      const T r = recip(sub);
+      const T f = dd[i] * r;
+      const T t = dd[i + 1];
       dd[i + 1] = du[i] - f * t;
       if (i < n - 2) {
         dl[i] = du[i + 1];
         du[i + 1] = -f * dl[i];
       } else {
-        dl[i] = 0.0;
+        dl[i] = T(0);
       }
       du[i] = t;
-      const double2 ty = y[i];
+      const V ty = y[i];
       y[i] = y[i + 1];
-      y[i + 1] = make_double2(ty.x - f * y[i + 1].x, ty.y - f * y[i + 1].y);
+      y[i + 1] = ty;
+      axpy_r<T>(y[i + 1], f, y[i]);
+      dd[i] = r;
     }
   }
-  if (dd[n - 1] == 0.0) dd[n - 1] = tiny;
-  y[n - 1].x /= dd[n - 1];
-  y[n - 1].y /= dd[n - 1];
+  if (dd[n - 1] == T(0)) dd[n - 1] = tiny;
+  scale_r<T>(y[n - 1], recip(dd[n - 1]));
   if (n > 1) {
-    y[n - 2].x = (y[n - 2].x - du[n - 2] * y[n - 1].x) / dd[n - 2];
-    y[n - 2].y = (y[n - 2].y - du[n - 2] * y[n - 1].y) / dd[n - 2];
+    axpy_r<T>(y[n - 2], du[n - 2], y[n - 1]);
+    scale_r<T>(y[n - 2], dd[n - 2]);
   }
   for (int i = n - 3; i >= 0; --i) {
-    y[i].x = (y[i].x - du[i] * y[i + 1].x - dl[i] * y[i + 2].x) / dd[i];
-    y[i].y = (y[i].y - du[i] * y[i + 1].y - dl[i] * y[i + 2].y) / dd[i];
+    axpy_r<T>(y[i], du[i], y[i + 1]);
+    axpy_r<T>(y[i], dl[i], y[i + 2]);
+    scale_r<T>(y[i], dd[i]);
   }
 }
 
@@ -1108,10 +1151,12 @@ __device__ void herm_matvec(const double* __restrict__ ainv, const float2* __res
 }
 
 // z <- H_k z for the reflectors of the workspace, k ascending (forward, Q^H z) or
-// descending (back, Q z); the reflectors' FP32 values are used exactly, in FP64. One warp.
-template <typename T, typename TA>
-__device__ void apply_q(const PointPtr<T, TA>& w, int n, double2* z, bool forward) {
+// descending (back, Q z), in the arithmetic V of z (float2 or double2); the reflectors'
+// stored values are used exactly. One warp.
+template <typename V, typename T, typename TA>
+__device__ void apply_q(const PointPtr<T, TA>& w, int n, typename C2<V>::type* z, bool forward) {
   using C = typename C2<T>::type;
+  using CV = typename C2<V>::type;
   const int lane = threadIdx.x & 31;
   if (n < 3) return;
   C cu[4], nu[4];
@@ -1120,14 +1165,14 @@ __device__ void apply_q(const PointPtr<T, TA>& w, int n, double2* z, bool forwar
   for (int s = 0; s + 2 < n; ++s) {
     const int k = forward ? s : n - 3 - s;
     if (s + 3 < n) load_refl(w, n, forward ? s + 1 : n - 4 - s, lane, nu, nt);  // the next one, early
-    const double tau = (double)ct;
-    if (tau != 0.0) {
+    const V tau = (V)ct;
+    if (tau != V(0)) {
       const int m = n - k - 1;
-      double2 acc = make_double2(0, 0), uu[4];
+      CV acc = mk<V>(0, 0), uu[4];
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const int i = lane + 32 * t;
-        uu[t] = make_double2(cu[t].x, cu[t].y);
+        uu[t] = mk<V>((V)cu[t].x, (V)cu[t].y);
         if (i < m) cmacc(acc, uu[t], z[k + 1 + i]);  // u^H z
       }
       acc.x = warp_sum(acc.x);
@@ -1136,7 +1181,7 @@ __device__ void apply_q(const PointPtr<T, TA>& w, int n, double2* z, bool forwar
       for (int t = 0; t < 4; ++t) {
         const int i = lane + 32 * t;
         if (i < m) {
-          const double2 tt = cmul(uu[t], acc);
+          const CV tt = cmul(uu[t], acc);
           z[k + 1 + i].x -= tau * tt.x;
           z[k + 1 + i].y -= tau * tt.y;
         }
@@ -1190,6 +1235,7 @@ __global__ void __launch_bounds__(32 * kRefineWarps, 4) tail_refine_kernel(
   double* s1 = yd + n;
   double* s2 = s1 + n;
   double* s3 = s2 + n;
+  float2* z32 = reinterpret_cast<float2*>(s1);  // FP32 work vector; s1 is scratch only inside the solve
   double2* dph = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(dd) + align16(6 * (size_t)n * sizeof(double)));
   double2* v = dph + n;
   double2* t1 = v + n;
@@ -1252,7 +1298,7 @@ __global__ void __launch_bounds__(32 * kRefineWarps, 4) tail_refine_kernel(
     if (lane == 0) {
       const T tiny = eps * fmax(tnorm, Lim<T>::tiny());
       for (int it = 0; it < 2; ++it) {
-        tridiag_solve(d, b, n, lam1, tiny, y, w1, w2, b2);  // b2 is free after the bisections
+        tridiag_solve_rcp(d, b, n, lam1, tiny, y, w1, w2, b2);  // b2 is free after the bisections
         T sc = 0;
         for (int i = 0; i < n; ++i) sc = fmax(sc, fabs(y[i]));
         if (!(sc > T(0)) || !isfinite(sc)) break;
@@ -1267,10 +1313,12 @@ __global__ void __launch_bounds__(32 * kRefineWarps, 4) tail_refine_kernel(
     yn = 1.0 / sqrt(warp_sum(yn));
     for (int i = lane; i < n; i += 32) {
       yd[i] *= yn;
-      v[i] = make_double2(dph[i].x * yd[i], dph[i].y * yd[i]);
+      z32[i] = make_float2((float)(dph[i].x * yd[i]), (float)(dph[i].y * yd[i]));
     }
     __syncwarp();
-    apply_q(w, n, v, false);
+    apply_q<float>(w, n, z32, false);
+    for (int i = lane; i < n; i += 32) v[i] = make_double2(z32[i].x, z32[i].y);
+    __syncwarp();
     // one correction step, then the check
     double lam = 0, rn = 0;
     for (int pass = 0; pass < 2; ++pass) {
@@ -1290,11 +1338,14 @@ __global__ void __launch_bounds__(32 * kRefineWarps, 4) tail_refine_kernel(
       rn = sqrt(warp_sum(r2) / vv);
       __syncwarp();
       if (pass == 1) break;
-      // dv = Q D P (R - lam I)^-1 P D^H Q^H r
-      apply_q(w, n, t1, true);
+      // dv = Q D P (R - lam I)^-1 P D^H Q^H r; the reflectors are applied in FP32 (the factors
+      // hold M only to FP32 accuracy anyway), the projected solve runs in FP64
+      for (int i = lane; i < n; i += 32) z32[i] = make_float2((float)t1[i].x, (float)t1[i].y);
+      __syncwarp();
+      apply_q<float>(w, n, z32, true);
       double2 pr = make_double2(0, 0);
       for (int i = lane; i < n; i += 32) {
-        t1[i] = cmulc(t1[i], dph[i]);  // D^H: times conj(delta_i)
+        t1[i] = cmulc(make_double2(z32[i].x, z32[i].y), dph[i]);  // D^H: times conj(delta_i)
         pr.x += yd[i] * t1[i].x;
         pr.y += yd[i] * t1[i].y;
       }
@@ -1302,19 +1353,21 @@ __global__ void __launch_bounds__(32 * kRefineWarps, 4) tail_refine_kernel(
       pr.y = warp_sum(pr.y);
       for (int i = lane; i < n; i += 32) { t1[i].x -= yd[i] * pr.x; t1[i].y -= yd[i] * pr.y; }
       __syncwarp();
-      if (lane == 0) tridiag_solve_c(dd, bd, n, lam, DBL_EPSILON * (double)tnorm + DBL_MIN, t1, s1, s2, s3);
+      if (lane == 0) tridiag_solve_rcp(dd, bd, n, lam, DBL_EPSILON * (double)tnorm + DBL_MIN, t1, s1, s2, s3);
       __syncwarp();
       pr = make_double2(0, 0);
       for (int i = lane; i < n; i += 32) { pr.x += yd[i] * t1[i].x; pr.y += yd[i] * t1[i].y; }
       pr.x = warp_sum(pr.x);
       pr.y = warp_sum(pr.y);
-      for (int i = lane; i < n; i += 32)
-        t1[i] = cmul(make_double2(t1[i].x - yd[i] * pr.x, t1[i].y - yd[i] * pr.y), dph[i]);
+      for (int i = lane; i < n; i += 32) {
+        const double2 x = cmul(make_double2(t1[i].x - yd[i] * pr.x, t1[i].y - yd[i] * pr.y), dph[i]);
+        z32[i] = make_float2((float)x.x, (float)x.y);
+      }
       __syncwarp();
-      apply_q(w, n, t1, false);
+      apply_q<float>(w, n, z32, false);
       double vn = 0;
       for (int i = lane; i < n; i += 32) {
-        v[i] = make_double2(v[i].x - t1[i].x, v[i].y - t1[i].y);
+        v[i] = make_double2(v[i].x - (double)z32[i].x, v[i].y - (double)z32[i].y);
         vn += v[i].x * v[i].x + v[i].y * v[i].y;
       }
       vn = 1.0 / sqrt(warp_sum(vn));
@@ -1376,24 +1429,31 @@ int occupancy(K kernel, int threads, size_t smem) {
   return occ;
 }
 
+// Most points of a sub-batch: its per-point workspace within 4 GiB (about 34,600 points at
+// N = 100), so that each launch has enough points to keep every SM busy to its end.
 template <typename T>
 int64_t sub_batch(int n) {
   const PointWs<T> w(n);  // FP64 sub-batches also fit the refined layout (it is smaller)
-  return (int64_t)std::max<size_t>(1024, std::min<size_t>(1 << 17, (size_t)(1ull << 30) / (w.bytes + 1)));
+  const int64_t def = (int64_t)std::max<size_t>(1024, std::min<size_t>(1 << 17, (size_t)(1ull << 32) / (w.bytes + 1)));
+  const int64_t cap = g_sub_batch_cap.load();
+  return cap > 0 ? std::min(cap, def) : def;
 }
 
 // Workspace of one sub-batch of `sub` points: per-point state of the widest arithmetic
-// used, route flags of the FP32 and FP64 passes, the list of routed points and its count.
+// used and the route flags of the FP32 and FP64 passes; then, for all `n_list` points of the
+// call, the list of points to redo in FP64 and its count. The redo runs once after every
+// sub-batch, so the few routed points of a call share launches instead of running a
+// nearly empty pass per sub-batch.
 struct SubWs {
   unsigned char* pts;
   uint8_t* sing;
   uint8_t* sing2;
   int32_t* list;
   int32_t* count;
-  static size_t bytes(int64_t sub, size_t point_bytes) {
-    return align16((size_t)sub * point_bytes) + 2 * align16((size_t)sub) + align16(4 * (size_t)sub) + 16;
+  static size_t bytes(int64_t sub, size_t point_bytes, int64_t n_list) {
+    return align16((size_t)sub * point_bytes) + 2 * align16((size_t)sub) + align16(4 * (size_t)n_list) + 16;
   }
-  SubWs(unsigned char* ws, int64_t sub, size_t point_bytes) {
+  SubWs(unsigned char* ws, int64_t sub, size_t point_bytes, int64_t n_list) {
     unsigned char* b = ws;
     pts = b;
     b += align16((size_t)sub * point_bytes);
@@ -1402,19 +1462,19 @@ struct SubWs {
     sing2 = b;
     b += align16((size_t)sub);
     list = reinterpret_cast<int32_t*>(b);
-    b += align16(4 * (size_t)sub);
+    b += align16(4 * (size_t)n_list);
     count = reinterpret_cast<int32_t*>(b);
   }
 };
 
-// List of the points to redo in FP64. `refined`: points singular in the (already FP64)
-// inverse are not redone.
-__global__ void route_kernel(const uint8_t* __restrict__ sing, int64_t nb, int32_t* __restrict__ list,
+// Appends the points of a sub-batch (global indices b0 + i) that are to be redone in FP64 to
+// the list. `refined`: points singular in the (already FP64) inverse are not redone.
+__global__ void route_kernel(const uint8_t* __restrict__ sing, int64_t nb, int64_t b0, int32_t* __restrict__ list,
                              int32_t* __restrict__ count, uint8_t* __restrict__ route, bool refined) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (int64_t)gridDim.x * blockDim.x) {
     const uint8_t f = sing[i];
     if (route) route[i] = f;
-    if (f && !(refined && f == kRouteSingular)) list[atomicAdd(count, 1)] = (int32_t)i;  // order is free
+    if (f && !(refined && f == kRouteSingular)) list[atomicAdd(count, 1)] = (int32_t)(b0 + i);  // order is free
   }
 }
 
@@ -1530,7 +1590,7 @@ int fast_supported(int n) { return n >= 2 && n <= kMaxFastN; }
 size_t fast_workspace_bytes(int64_t n_pc, int n) {
   const int64_t s32 = std::min<int64_t>(n_pc, sub_batch<float>(n));
   const int64_t s64 = std::min<int64_t>(n_pc, sub_batch<double>(n));
-  return std::max(SubWs::bytes(s32, PointWs<float>(n).bytes), SubWs::bytes(s64, point_bytes_max(n)));
+  return std::max(SubWs::bytes(s32, PointWs<float>(n).bytes, n_pc), SubWs::bytes(s64, point_bytes_max(n), n_pc));
 }
 
 int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, float cond_max, float2* ph,
@@ -1544,9 +1604,14 @@ int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, flo
   auto* ws = static_cast<unsigned char*>(workspace);
   // a mixed or refined sub-batch must hold its points in FP64 when all of them are routed
   const bool wide = f64 || mixed || refine;
-  const int64_t sub = std::min<int64_t>(n_pc, wide ? sub_batch<double>(n) : sub_batch<float>(n));
-  const SubWs w(ws, sub, wide ? point_bytes_max(n) : PointWs<float>(n).bytes);
+  // sub-batches of equal size (none left nearly empty at the end)
+  const int64_t cap = wide ? sub_batch<double>(n) : sub_batch<float>(n);
+  const int64_t nsub = (n_pc + cap - 1) / cap;
+  const int64_t sub = nsub > 0 ? (n_pc + nsub - 1) / nsub : 0;
+  const SubWs w(ws, sub, wide ? point_bytes_max(n) : PointWs<float>(n).bytes, n_pc);
   const int64_t npairs = (int64_t)n * (n - 1) / 2;
+  const bool routed = mixed || refine;
+  if (routed) MR_CUDA_TRY(cudaMemsetAsync(w.count, 0, sizeof(int32_t), s));
   for (int64_t b0 = 0; b0 < n_pc; b0 += sub) {
     const int64_t nb = std::min<int64_t>(sub, n_pc - b0);
     const float2* c = coh + b0 * npairs;
@@ -1561,17 +1626,24 @@ int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, flo
     } else {
       rc = refine ? run_refine_pass(c, all, n, ref, p, q, t, w.pts, w.sing, (double)cond_max, s)
                   : run_pass<float>(c, all, n, ref, p, q, t, w.pts, w.sing, mixed ? cond_max : 0.f, s);
-      if (!rc && (mixed || refine)) {
-        MR_CUDA_TRY(cudaMemsetAsync(w.count, 0, sizeof(int32_t), s));
+      if (!rc && routed) {
         const int grid = (int)std::min<int64_t>((nb + 255) / 256, (int64_t)sm_count() * 8);
-        route_kernel<<<grid, 256, 0, s>>>(w.sing, nb, w.list, w.count, route ? route + b0 : nullptr, refine);
+        route_kernel<<<grid, 256, 0, s>>>(w.sing, nb, b0, w.list, w.count, route ? route + b0 : nullptr, refine);
         rc = check_launch("emi route");
-        if (!rc) rc = run_pass<double>(c, PointSet{w.list, w.count, nb}, n, ref, p, q, t, w.pts, w.sing2, 0.f, s);
       } else if (!rc && route) {
         MR_CUDA_TRY(cudaMemsetAsync(route + b0, 0, (size_t)nb, s));
       }
     }
     if (rc) return rc;
+  }
+  // the routed points of every sub-batch, in FP64, in windows of `sub` list entries (the
+  // count is known only on the device: windows past it exit at once)
+  if (routed) {
+    for (int64_t l0 = 0; l0 < n_pc; l0 += sub) {
+      const int rc = run_pass<double>(coh, PointSet{w.list, w.count, sub, nullptr, l0}, n, ref, ph, quality, tcoh,
+                                      w.pts, w.sing2, 0.f, s);
+      if (rc) return rc;
+    }
   }
   return MR_OK;
 }

@@ -77,7 +77,7 @@ void note_launches(int k) { g_launches.fetch_add((uint64_t)k, std::memory_order_
 
 extern "C" uint64_t mr_kernel_launches(void) { return mr::g_launches.load(std::memory_order_relaxed); }
 
-extern "C" int mr_abi_version(void) { return 3; }
+extern "C" int mr_abi_version(void) { return 4; }
 
 // ---------------------------------------------------------------- per-kernel timing
 

@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_version_and_sizes():
     lib = _lib.load()
-    assert lib.mr_abi_version() == 3
+    assert lib.mr_abi_version() == 4
     assert lib.mr_ks_workspace_bytes(200, 200, 17) == 200 * 200 * 20 * 4
     assert lib.mr_ks_workspace_bytes(0, 200, 17) == 0
     assert lib.mr_ds_extract_workspace_bytes(4096) == 4 * 8
@@ -60,7 +60,7 @@ C_HOST = r"""
 
 int main(void) {
   /* host-side paths only: no device memory, no kernel */
-  if (mr_abi_version() != 3) return 1;
+  if (mr_abi_version() != 4) return 1;
   if (mr_gamma_sample_bytes(MR_GAMMA_FCOMPLEX) != 8) return 2;
   if (mr_ks_workspace_bytes(100, 100, 17) == 0) return 3;
   if (mr_ds_chain_workspace_bytes(64, 64, 20, 2, 3, 1000) == 0) return 4;
@@ -97,3 +97,20 @@ def test_kernel_timing_empty_without_launches():
     assert _lib.kernel_timing() == {}
     lib.mr_set_kernel_timing(0)
     assert lib.mr_kernel_timing(-1, None, None, None) == 0
+
+
+def test_emi_sub_batch_cap_sizes_the_workspace():
+    """A smaller EMI sub-batch lowers the workspace; a workspace sized before a larger cap
+    is rejected before any device work; negative caps are invalid."""
+    lib = _lib.load()
+    full = lib.mr_emi_workspace_bytes(100000, 100)
+    assert lib.mr_set_emi_sub_batch(4096) == 0
+    try:
+        small = lib.mr_emi_workspace_bytes(100000, 100)
+        assert small < full / 4
+        assert lib.mr_set_emi_sub_batch(0) == 0
+        assert lib.mr_emi_workspace_bytes(100000, 100) == full
+        assert lib.mr_emi(16, 100000, 100, 0, 0, 16, 16, None, 16, small, None) == _lib.MR_ERR_WORKSPACE
+        assert lib.mr_set_emi_sub_batch(-1) == _lib.MR_ERR_INVALID
+    finally:
+        lib.mr_set_emi_sub_batch(0)

@@ -275,6 +275,118 @@ def test_chain_refine_route(cuda):
     assert torch.equal(res.ph[again], ref.ph[again])
 
 
+@pytest.mark.parametrize("n", [2, 3, 4, 5, 15, 16, 17, 18, 31, 32, 33, 47, 64, 65, 99, 100, 101, 112, 113, 127, 128])
+def test_emi_refine_every_block_shape(cuda, n):
+    """The refined EMI (pivot-pair sweep, FP32 reduction, FP64 correction) at every parity and
+    16-block boundary of N: kept points agree with the FP64 run within the refinement bound,
+    recomputed points equal it bit for bit."""
+    rng = np.random.default_rng(n)
+    looks = 2 * n + 8
+    z = rng.normal(size=(96, looks, n)) + 1j * rng.normal(size=(96, looks, n))
+    C = np.einsum("pli,plj->pij", z, z.conj())
+    d = np.sqrt(np.einsum("pii->pi", C).real)
+    C = C / (d[:, :, None] * d[:, None, :])
+    r, s = np.triu_indices(n, 1)
+    coh = C[:, r, s].astype(np.complex64)
+    ph, q, route = mb.emi(coh, precision="refine", return_route=True)
+    ph64, q64 = mb.emi(coh, precision="fp64")
+    kept, redone = route == 0, route == 1
+    assert kept.mean() > 0.5
+    err = np.abs(np.angle(ph * np.conj(ph64))).max(-1)
+    assert np.all(err[kept] <= 2e-4), err[kept].max()
+    np.testing.assert_array_equal(ph[redone].view(np.int32), ph64[redone].view(np.int32))
+    np.testing.assert_allclose(q[kept], q64[kept], rtol=1e-4, atol=1e-5)
+
+
+def test_refine_reruns_across_sub_batches(cuda):
+    """More points than one sub-batch (capped at 4,096 points here): the points routed to FP64
+    in every sub-batch are recomputed together after the last one. Copies of a point give the
+    same bits and route wherever they fall; with a bound nothing meets, every point is
+    recomputed (a list three sub-batches long) and equals the FP64 run."""
+    from moraine_b200 import _lib
+    cfg = CONFIGS["c2"].scaled(nlines=40, width=40)
+    z = make_stack(cfg).numpy()
+    p = O.ks_test(O.intensity(z), cfg.az_half_win, cfg.r_half_win)
+    is_shp, num = O.select_shp(p, cfg.p_max)
+    idx, pc = O.ds_candidates(is_shp, num, 1)
+    base = O.emperical_co_pc(z, idx, pc).astype(np.complex64)
+    reps = -(-12000 // base.shape[0])
+    coh = np.tile(base, (reps, 1))
+    lib = _lib.load()
+    assert lib.mr_set_emi_sub_batch(4096) == 0
+    try:
+        assert coh.shape[0] > 2 * 4096
+        ph, q, route = mb.emi(coh, precision="refine", return_route=True)
+        m = base.shape[0]
+        for k in range(1, reps):
+            np.testing.assert_array_equal(ph[k * m:(k + 1) * m].view(np.int32), ph[:m].view(np.int32))
+            np.testing.assert_array_equal(route[k * m:(k + 1) * m], route[:m])
+        ph64, q64 = mb.emi(coh, precision="fp64")
+        redone = route == 1
+        np.testing.assert_array_equal(ph[redone].view(np.int32), ph64[redone].view(np.int32))
+        ph_all, q_all, r_all = mb.emi(coh, precision="refine", return_route=True, refine_tol=1e-30)
+        assert np.all(r_all != 0)
+        ok = r_all == 1  # route 2: singular in FP64 as well, NaN
+        assert ok.mean() > 0.99
+        np.testing.assert_array_equal(ph_all[ok].view(np.int32), ph64[ok].view(np.int32))
+        np.testing.assert_array_equal(q_all[ok].view(np.int32), q64[ok].view(np.int32))
+        # the same bits as without the cap
+        assert lib.mr_set_emi_sub_batch(0) == 0
+        ph_one, _, route_one = mb.emi(coh, precision="refine", return_route=True)
+        np.testing.assert_array_equal(ph_one.view(np.int32), ph.view(np.int32))
+        np.testing.assert_array_equal(route_one, route)
+    finally:
+        lib.mr_set_emi_sub_batch(0)
+
+
+def test_refine_small_pivot_goes_to_fp64(cuda):
+    """A point whose |Gamma| meets a tiny pivot in natural order (|gamma_01|^2 within 1e-10
+    of 1, so the second pivot of the symmetric sweep is below 1e-9) is flagged by the sweep
+    and recomputed by the pivoted FP64 path: the same bits as the FP64 run."""
+    rng = np.random.default_rng(5)
+    n = 12
+    th = np.linspace(0.1, 1.5, 200001)  # a complex64 value of modulus 1 - O(1e-11)
+    re, im = np.cos(th).astype(np.float32), np.sin(th).astype(np.float32)
+    deficit = 1 - (re.astype(np.float64) ** 2 + im.astype(np.float64) ** 2)
+    k = int(np.flatnonzero((deficit > 1e-11) & (deficit < 1e-10))[0])
+    g = np.full((n, n), 0.3) + 0.05 * rng.random((n, n))
+    g = (g + g.T) / 2
+    np.fill_diagonal(g, 1.0)
+    ph = np.exp(1j * rng.uniform(-np.pi, np.pi, n))
+    G = g * np.outer(ph, ph.conj())
+    G[0, 1] = complex(re[k], im[k])
+    r, s = np.triu_indices(n, 1)
+    ok = rng.normal(size=(40, n)) + 1j * rng.normal(size=(40, n))  # an ordinary point beside it
+    C = ok.conj().T @ ok
+    d = np.sqrt(np.diag(C).real)
+    Cn = C / np.outer(d, d)
+    coh = np.stack([G[r, s], Cn[r, s]]).astype(np.complex64)
+    assert coh[0, 0] == np.complex64(complex(re[k], im[k]))
+    ph_r, q_r, route = mb.emi(coh, precision="refine", return_route=True)
+    ph64, q64 = mb.emi(coh, precision="fp64")
+    assert route[0] == 1
+    np.testing.assert_array_equal(ph_r[0].view(np.int32), ph64[0].view(np.int32))
+    np.testing.assert_array_equal(q_r[:1].view(np.int32), q64[:1].view(np.int32))
+    assert np.all(np.isfinite(ph_r[0]))
+
+
+def test_kernel_timing_names_the_chain_kernels(cuda):
+    from moraine_b200 import _lib
+    cfg = CONFIGS["c2"].scaled(nlines=48, width=48)
+    z = make_stack(cfg, device=cuda)
+    ch = DsChain(48, 48, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, 1, device=cuda,
+                 precision="fp64", emi_precision="refine")
+    ch.run(z)
+    lib = _lib.load()
+    lib.mr_set_kernel_timing(1)
+    ch.run(z)
+    torch.cuda.synchronize()
+    kt = _lib.kernel_timing()
+    lib.mr_set_kernel_timing(0)
+    for name in ("ks sort keys", "ks merge", "gram fp64", "emi sweep fp64", "emi reduce fp32", "emi refine tail"):
+        assert name in kt and kt[name][0] > 0 and kt[name][1] >= 1, (name, kt)
+
+
 def test_chain_mixed_route(cuda):
     cfg = CONFIGS["c3"].scaled(nlines=24, width=24, nimages=64)
     z = make_stack(cfg, device=cuda)
