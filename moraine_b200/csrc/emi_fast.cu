@@ -1,24 +1,25 @@
-// EMI for N <= 128, one CTA of 256 threads per point.
+// EMI for N <= 128 (moraine/pl.py:46-77: M = inv(|Gamma|) o Gamma, its smallest eigenpair,
+// phases referred to image `ref`, fused temporal coherence), in sub-batches of points.
 //
-// Gauss-Jordan in registers (gj_tile): the padded 16NB x 16NB matrix |Gamma| is held by a
-//   16 x 16 thread grid, thread (tx, ty) owning rows ty + 16 ib and columns tx + 16 jb.
-//   Rows are never swapped: at step k the half-warp owning column k finds the pivot row
-//   p_k among the rows not yet used (largest |a|) and publishes column k through a
-//   double-buffered shared vector; every column group fetches row p_k by shuffles. One
-//   barrier per step. The result R satisfies inv[k][p_j] = R[p_k][j].
-// Householder reduction (tridiag_packed): M = inv(|Gamma|) o Gamma as a packed lower
-//   triangle in shared memory; step k's rank-2 update is fused with the product of step
-//   k+1, mirrored row pairs give every thread the same work.
-// Three kernels per sub-batch of points, in FP32 or FP64 (template T):
-//   inverse_kernel<T, NB>  inv(|Gamma|) in registers -> workspace (lower triangle, packed);
-//   reduce_kernel<T>       M in shared memory, Householder reduction -> workspace (d, e, tau,
-//                          reflectors);
-//   tail_kernel<T>         one warp per point: smallest eigenvalue by Sturm multisection,
-//                          inverse iteration on the real tridiagonal, back-transformation,
-//                          normalisation to the reference image, temporal coherence.
-// Splitting by resource lets each stage run at its own occupancy: the serial, O(N)
-// tail of many points overlaps on one SM, and the register-bound inverse is not held
-// back by the shared memory of the reduction.
+// Kernels, each at its own occupancy (the register-bound inverse is not held back by the
+// shared memory of the reduction, and the serial O(N) tails of many points overlap on an SM):
+//   inverse_kernel<T, NB>  inv(|Gamma|) by Gauss-Jordan with partial pivoting in registers
+//                          (gj_tile): the padded 16NB x 16NB matrix on a 16 x 16 thread grid,
+//                          rows never swapped, one barrier per step; the result stored
+//                          upper-packed in the workspace. FP32 and FP64 EMI, and the FP64
+//                          recomputation of routed points.
+//   sweep_kernel<NB>       inv(|Gamma|) in FP64 for the refined EMI: the symmetric sweep, two
+//                          pivots per barrier, only the lower triangle held.
+//   reduce_kernel<T, TA>   M in shared memory as a packed lower triangle, Householder
+//                          reduction to a real tridiagonal (tridiag_packed) -> workspace (d, e,
+//                          tau, reflectors).
+//   tail_kernel<T, TA>     one warp per point: smallest eigenvalue by Sturm multisection,
+//                          inverse iteration, back-transformation, normalisation, temporal
+//                          coherence.
+//   tail_refine_kernel     the refined EMI's tail: FP32 eigenpair of the tridiagonal, one FP64
+//                          Newton correction and an FP64 error bound that routes the points
+//                          it does not certify to FP64.
+//   route_kernel           collects the points to recompute in FP64 over all sub-batches.
 #include <algorithm>
 #include <atomic>
 
@@ -451,15 +452,19 @@ __device__ void tridiag_packed(const TriShared<T>& s, int n) {
 }
 
 
-// acc += a b
+// acc += a b (one FMA per product)
 template <typename C> __device__ __forceinline__ void cmac(C& acc, C a, C b) {
-  acc.x += a.x * b.x - a.y * b.y;
-  acc.y += a.x * b.y + a.y * b.x;
+  acc.x += a.x * b.x;
+  acc.x -= a.y * b.y;
+  acc.y += a.x * b.y;
+  acc.y += a.y * b.x;
 }
 // acc += conj(a) b
 template <typename C> __device__ __forceinline__ void cmacc(C& acc, C a, C b) {
-  acc.x += a.x * b.x + a.y * b.y;
-  acc.y += a.x * b.y - a.y * b.x;
+  acc.x += a.x * b.x;
+  acc.x += a.y * b.y;
+  acc.y += a.x * b.y;
+  acc.y -= a.y * b.x;
 }
 template <typename C> __device__ __forceinline__ C shfl_xor_c(C v, int o) {
   v.x = __shfl_xor_sync(0xffffffffu, v.x, o);
