@@ -154,6 +154,18 @@ def dtype_of(gram: str, emi: str) -> str:
 # points; FP32: 4.195 GB / 17,485 points); the traffic scales with the points processed
 EMI_TRAFFIC_PER_POINT = {(100, "fp64"): 356_500, (100, "fp32"): 239_900}
 
+# DRAM bytes per unit of one kernel (dram__bytes_read.sum + dram__bytes_write.sum of one launch
+# / the units it processed), from one-kernel ncu captures on the 512 x 512 x 100 crop of the c2
+# scene model (profiles/*_c2_512.md); the traffic of these kernels scales with the units, so a
+# full-size launch gets units x bytes. Keyed by (kernel, N); DS points, pixels for the KS merge.
+KERNEL_TRAFFIC_PER_UNIT = {
+    ("emi reduce fp32", 100): (2.768748e9 + 1.384547e9) / 34_510,   # prof512_reduce_f32c
+    ("emi refine tail", 100): (10.324045e9 + 31.297536e6) / 34_510,  # prof512_tail_refine_c
+    ("emi sweep fp64", 100): (1.368710e9 + 1.348463e9) / 34_510,     # prof512_sweep2
+    ("gram fp64", 100): (1.502556e9 + 2.682337e9) / 69_019,          # prof512_gram_b
+    ("ks merge", 100): (109.437696e6 + 38.131456e6) / 262_144,       # prof512_ks_kept
+}
+
 
 def fp32_simt_peak(dev) -> float:
     """FP32 FMA-pipe reference rate in TFLOP/s: cuBLAS SGEMM 8192^3 with TF32 off, best of 5."""
@@ -241,7 +253,8 @@ def kernel_rooflines(cfg, ktimes: dict, n_ds: int, res, peaks: dict, fp32: float
     per unit, and the bound:
       ks sort keys      pixel: 4N bytes in, 4K out (K = keys per pixel)          HBM
       ks merge          pixel: 4N + W + 4 bytes (keys in, mask and count out)     HBM (as asked;
-                        its real limit is integer issue: W(2N-1) merge steps per pixel)
+                        its real limit is shared memory: the bank conflicts of its
+                        data-dependent merge reads, W(2N-1) merge steps per pixel)
       gram fp32/fp64    DS point: 8 S Q + 3 S N flops (S its SHP count)          FP32 / FP64 pipe
       emi inverse/sweep DS point: N^3/3 + N^3 flops (factorisation and inverse of |Gamma|)
       emi reduce        DS point: 4N^3/3 flops (the complex factorisation of M)
@@ -265,6 +278,12 @@ def kernel_rooflines(cfg, ktimes: dict, n_ds: int, res, peaks: dict, fp32: float
             continue
         per = ms / launches
         ent = {"kernel": name, "launches": launches, "ms_total": ms, "ms_per_launch": per, "traffic": None}
+        tpu = KERNEL_TRAFFIC_PER_UNIT.get((name, n))
+        if tpu:
+            units = npix if name == "ks merge" else n_ds
+            ent["traffic"] = tpu * units / launches
+            ent["traffic_source"] = ("ncu DRAM bytes per unit on a 512 x 512 crop of the same scene model, "
+                                     "scaled to the units of a launch")
         if name == "ks sort keys":
             byts = npix * (4 * n + 4 * ((n + 4) & ~3)) / launches
             ent.update(bound="hbm", unit="GB/s", achieved=byts / (per / 1e3) / 1e9, peak=hbm,

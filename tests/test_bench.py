@@ -46,3 +46,34 @@ def test_ours_arm_rejects_zero_warmup():
     out = subprocess.run([sys.executable, str(REPO / "bench.py"), "--warmup", "0", "--steps", "1"],
                          capture_output=True, text=True, timeout=120, cwd=REPO)
     assert out.returncode == 2 and "--warmup must be at least 1" in out.stderr
+
+
+def test_kernel_rooflines_traffic_and_work():
+    """Per-kernel rooflines on the host: the algorithmic work per unit, and the DRAM traffic of
+    a launch scaled from the one-kernel captures' bytes per unit."""
+    import importlib.util
+    from types import SimpleNamespace
+
+    import pytest
+    import torch
+
+    spec = importlib.util.spec_from_file_location("bench_mod", REPO / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    cfg = SimpleNamespace(nimages=100, nlines=8, width=8, az_win=11, r_win=21)
+    res = SimpleNamespace(idx=torch.tensor([[0, 0], [1, 1], [2, 2]], dtype=torch.int32),
+                          shp_num=torch.full((8, 8), 50, dtype=torch.int32))
+    kt = {"emi reduce fp32": (6.0, 3), "emi sweep fp64": (3.0, 3), "ks merge": (1.0, 1), "gram fp64": (2.0, 1),
+          "emi refine tail": (1.5, 3)}
+    out = bench.kernel_rooflines(cfg, kt, 3, res, {"hbm_gbs": 6547.2, "source": "measured"}, 64.0)
+    per = bench.KERNEL_TRAFFIC_PER_UNIT
+    assert out["emi reduce fp32"]["traffic"] == pytest.approx(per[("emi reduce fp32", 100)] * 3 / 3)
+    assert out["ks merge"]["traffic"] == pytest.approx(per[("ks merge", 100)] * 64)
+    assert out["gram fp64"]["traffic"] == pytest.approx(per[("gram fp64", 100)] * 3)
+    red, swp = out["emi reduce fp32"], out["emi sweep fp64"]
+    assert red["algorithmic_flops_per_unit"] == pytest.approx(4 * 100 ** 3 / 3)
+    assert red["executed_flops_per_unit"] == pytest.approx(16 * 100 ** 3 / 3)
+    assert swp["algorithmic_flops_per_unit"] == pytest.approx(4 * 100 ** 3 / 3) and swp["bound"] == "fp64-simt"
+    assert out["emi refine tail"]["bound"] == "fp64-simt"
+    # achieved = work of a launch / its mean duration (2 ms for one DS point per launch)
+    assert red["achieved"] == pytest.approx(4 * 100 ** 3 / 3 / 2e-3 / 1e12)
