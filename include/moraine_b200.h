@@ -281,7 +281,8 @@ int mr_emi_routed(const mr_complex64* coh, int64_t n_pc, int nimages, int ref, d
  * FP32 factors M ~ Q T Q^H with T's own eigenvector projected out. The refined pair is
  * checked in FP64: residual r', gap g = lambda_2(T) - lambda and smallest component
  * min|v_i| bound the phase error of every date by |r'| / (g min|v_i|); points whose
- * bound exceeds tol are recomputed in FP64. route (may be NULL, n_pc bytes) receives per
+ * bound exceeds tol (decided by a Sturm count of T at the shift where it would equal tol)
+ * are recomputed in FP64. route (may be NULL, n_pc bytes) receives per
  * point 0 = refined, 1 = recomputed in FP64, 2 = |Gamma| singular in FP64 (NaN output);
  * 1 for every point when nimages > 128 (FP64 throughout). Same computation as
  * moraine.pl.emi (moraine/pl.py:68-77); the refinement has no reference counterpart. */

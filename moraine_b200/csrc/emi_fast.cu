@@ -1308,7 +1308,6 @@ __global__ void __launch_bounds__(32 * kRefineWarps, 4) tail_refine_kernel(
     lo -= pad;
     hi += pad;
     const T lam1 = multisect(d, b2, n, lo, hi, 1, pivmin, 64);
-    const T lam2 = n > 1 ? multisect(d, b2, n, lo, hi, 2, pivmin, 6) : hi;
     // eigenvector y of R by inverse iteration (FP32, lane 0)
     for (int i = lane; i < n; i += 32) y[i] = T(1) + T(0.25) * (T)((i * 37) % 11) / T(11);
     __syncwarp();
@@ -1396,11 +1395,18 @@ __global__ void __launch_bounds__(32 * kRefineWarps, 4) tail_refine_kernel(
     for (int i = lane; i < n; i += 32) vmin = fmin(vmin, sqrt(v[i].x * v[i].x + v[i].y * v[i].y));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) vmin = fmin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
-    const double gap = (double)lam2 - lam - 4.0 * (double)eps * (double)n * (double)tnorm;
-    const double bound = rn / (gap * vmin);
+    // |r'| / (gap min|v_i|) <= tol with gap = lambda_2(R) - lam - margin holds exactly when
+    // lambda_2(R) >= sig = lam + margin + |r'| / (tol min|v_i|): one Sturm count at sig
+    // (rounded up to FP32) answers it, without locating lambda_2
+    const double sig = lam + 4.0 * (double)eps * (double)n * (double)tnorm + rn / (tol * vmin);
+    for (int i = lane; i + 1 < n; i += 32) b2[i] = b[i] * b[i];  // b2 was the solves' scratch
+    __syncwarp();
+    float sg = (float)sig;
+    if ((double)sg < sig) sg = nextafterf(sg, 3.4e38f);
+    const bool gap_ok = sig < 3.0e38 && sturm_count(d, b2, n, (T)sg, pivmin) <= 1;  // NaN: false
     const bool singular = (sing[pt] & kRouteSingular) != 0;
     const bool small_pivot = (sing[pt] & kRouteCond) != 0;  // the sweep's inverse is not trusted
-    const bool ok = singular || (!small_pivot && gap > 0.0 && bound <= tol);
+    const bool ok = singular || (!small_pivot && gap_ok);
     // normalise to the reference image
     const double2 zr = v[ref];
     for (int i = lane; i < n; i += 32) {
