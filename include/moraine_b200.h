@@ -329,7 +329,8 @@ int mr_ds_chain(const mr_complex64* rslc, int nlines, int width, int nimages, in
 /* mr_ds_chain without the host synchronisation, for capture in a CUDA graph: the DS count
  * goes to n_ds_dev (device memory) and the kernels read it there, processing every batch
  * that max_ds allows (batches past the count do no work). Only stream-ordered work, no
- * allocation. Limits: nimages <= 128, gram and emi precision MR_PREC_FP32 or MR_PREC_FP64.
+ * allocation. Limits: nimages <= 128, gram precision MR_PREC_FP32 or MR_PREC_FP64, emi
+ * precision MR_PREC_FP32, MR_PREC_FP64 or MR_PREC_REFINE (tolerance MR_EMI_REFINE_TOL).
  * Points past max_ds are not processed: compare *n_ds_dev with max_ds afterwards. Same
  * results as mr_ds_chain. No reference counterpart. */
 int mr_ds_chain_async(const mr_complex64* rslc, int nlines, int width, int nimages, int az_half_win,

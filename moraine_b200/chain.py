@@ -22,6 +22,7 @@ from dataclasses import dataclass, field
 import torch
 
 from . import _dev, _lib
+from .pl import EMI_REFINE_TOL
 
 
 @dataclass
@@ -44,7 +45,7 @@ class DsChain:
                  p_max: float = 0.05, min_shp: int = 50, precision: str = "fp32", batch: int | None = None,
                  device=None, timing: bool = False, emi_precision: str | None = None,
                  cond_max: float = 1.0e4, graph: bool = False, ks_input: str = "intensity",
-                 refine_tol: float = 1.0e-4):
+                 refine_tol: float = EMI_REFINE_TOL):
         self.device = torch.device(device) if device is not None else _dev.require_cuda()
         if ks_input not in _lib.KS_INPUT:
             raise ValueError(f"ks_input must be 'intensity' or 'amplitude', not {ks_input!r}")
@@ -91,8 +92,13 @@ class DsChain:
         self.graph = bool(graph)
         self._graph = None
         if self.graph:
-            if nimages > 128 or precision not in ("fp32", "fp64") or emi_precision not in ("fp32", "fp64"):
-                raise ValueError("DsChain(graph=True) needs nimages <= 128 and fp32/fp64 arithmetic")
+            if (nimages > 128 or precision not in ("fp32", "fp64")
+                    or emi_precision not in ("fp32", "fp64", "refine")):
+                raise ValueError("DsChain(graph=True) needs nimages <= 128, an fp32/fp64 Gram and fp32, fp64 or "
+                                 "refined EMI")
+            if emi_precision == "refine" and self.refine_tol != EMI_REFINE_TOL:
+                raise ValueError("DsChain(graph=True) refines to the library's default tolerance "
+                                 f"({EMI_REFINE_TOL} rad)")
             self.x = torch.empty((nlines, width, nimages), dtype=torch.complex64, device=d)
             gbytes = lib.mr_ds_chain_workspace_bytes(nlines, width, nimages, az_half_win, r_half_win, self.batch)
             self.g_ws = _dev.workspace(gbytes + 256, d)

@@ -132,8 +132,8 @@ extern "C" int mr_ds_chain_async(const mr_complex64* rslc, int nlines, int width
   if (nimages > 128)
     return fail(MR_ERR_UNSUPPORTED, "ds_chain_async: nimages %d > 128 (use mr_ds_chain)", nimages);
   if ((gram_precision != MR_PREC_FP32 && gram_precision != MR_PREC_FP64) ||
-      (emi_precision != MR_PREC_FP32 && emi_precision != MR_PREC_FP64))
-    return fail(MR_ERR_UNSUPPORTED, "ds_chain_async: gram and emi precision must be FP32 or FP64");
+      (emi_precision != MR_PREC_FP32 && emi_precision != MR_PREC_FP64 && emi_precision != MR_PREC_REFINE))
+    return fail(MR_ERR_UNSUPPORTED, "ds_chain_async: gram precision must be FP32 or FP64, emi FP32, FP64 or REFINE");
   const int az_win = 2 * az_half_win + 1, r_win = 2 * r_half_win + 1, win = az_win * r_win;
   const size_t need = mr_ds_chain_workspace_bytes(nlines, width, nimages, az_half_win, r_half_win, batch);
   if (!workspace || workspace_bytes < need)

@@ -300,10 +300,11 @@ int emi_counted(const float2* coh, int64_t n_max, const int64_t* dcount, int64_t
                 float2* ph, float* quality, float* tcoh, void* workspace, size_t workspace_bytes, cudaStream_t s) {
   if (n_max <= 0) return MR_OK;
   if (!emi::fast_supported(n)) return fail(MR_ERR_UNSUPPORTED, "emi: device-counted points need nimages <= 128");
-  if (precision != MR_PREC_FP32 && precision != MR_PREC_FP64)
-    return fail(MR_ERR_UNSUPPORTED, "emi: device-counted points run in FP32 or FP64");
+  if (precision != MR_PREC_FP32 && precision != MR_PREC_FP64 && precision != MR_PREC_REFINE)
+    return fail(MR_ERR_UNSUPPORTED, "emi: device-counted points run in FP32, FP64 or refined");
   if (!workspace || workspace_bytes < mr_emi_workspace_bytes(n_max, n))
     return fail(MR_ERR_WORKSPACE, "emi: workspace too small");
-  return emi::fast_run(coh, n_max, n, 0, precision, 0.f, ph, quality, tcoh, nullptr, workspace, s, dcount, doff);
+  const float tol = precision == MR_PREC_REFINE ? (float)MR_EMI_REFINE_TOL : 0.f;  // the refinement's bound
+  return emi::fast_run(coh, n_max, n, 0, precision, tol, ph, quality, tcoh, nullptr, workspace, s, dcount, doff);
 }
 }  // namespace mr

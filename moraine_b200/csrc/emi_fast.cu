@@ -1491,9 +1491,16 @@ struct SubWs {
 };
 
 // Appends the points of a sub-batch (global indices b0 + i) that are to be redone in FP64 to
-// the list. `refined`: points singular in the (already FP64) inverse are not redone.
+// the list. `refined`: points singular in the (already FP64) inverse are not redone. With a
+// device-held point count (dcount, the sub-batch starting at point doff of it) only the
+// points below it are read.
 __global__ void route_kernel(const uint8_t* __restrict__ sing, int64_t nb, int64_t b0, int32_t* __restrict__ list,
-                             int32_t* __restrict__ count, uint8_t* __restrict__ route, bool refined) {
+                             int32_t* __restrict__ count, uint8_t* __restrict__ route, bool refined,
+                             const int64_t* __restrict__ dcount, int64_t doff) {
+  if (dcount) {
+    const int64_t c = *dcount - doff;
+    nb = c < 0 ? 0 : (c < nb ? c : nb);
+  }
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (int64_t)gridDim.x * blockDim.x) {
     const uint8_t f = sing[i];
     if (route) route[i] = f;
@@ -1622,8 +1629,7 @@ int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, flo
   const bool f64 = precision == MR_PREC_FP64;
   const bool mixed = precision == MR_PREC_MIXED;
   const bool refine = precision == MR_PREC_REFINE;
-  if (dcount && (mixed || refine))
-    return fail(MR_ERR_UNSUPPORTED, "emi: device-counted points run in FP32 or FP64");
+  if (dcount && mixed) return fail(MR_ERR_UNSUPPORTED, "emi: device-counted points run in FP32, FP64 or refined");
   auto* ws = static_cast<unsigned char*>(workspace);
   // a mixed or refined sub-batch must hold its points in FP64 when all of them are routed
   const bool wide = f64 || mixed || refine;
@@ -1651,7 +1657,8 @@ int fast_run(const float2* coh, int64_t n_pc, int n, int ref, int precision, flo
                   : run_pass<float>(c, all, n, ref, p, q, t, w.pts, w.sing, mixed ? cond_max : 0.f, s);
       if (!rc && routed) {
         const int grid = (int)std::min<int64_t>((nb + 255) / 256, (int64_t)sm_count() * 8);
-        route_kernel<<<grid, 256, 0, s>>>(w.sing, nb, b0, w.list, w.count, route ? route + b0 : nullptr, refine);
+        route_kernel<<<grid, 256, 0, s>>>(w.sing, nb, b0, w.list, w.count, route ? route + b0 : nullptr, refine,
+                                          dcount, doff + b0);
         rc = check_launch("emi route");
       } else if (!rc && route) {
         MR_CUDA_TRY(cudaMemsetAsync(route + b0, 0, (size_t)nb, s));

@@ -623,14 +623,14 @@ def test_maximum_sizes(cuda):
         mb.ks_test(x, 32, 32)  # 65 x 65 = 4225 cells
 
 
-@pytest.mark.parametrize("prec", ["fp32", "fp64"])
-def test_chain_in_cuda_graph(cuda, prec):
-    """The chain captured once in a CUDA graph and replayed on two stacks equals the plain chain."""
+@pytest.mark.parametrize("prec,emi_prec", [("fp32", None), ("fp64", None), ("fp64", "refine")])
+def test_chain_in_cuda_graph(cuda, prec, emi_prec):
+    """The chain captured once in a CUDA graph and replayed on two stacks equals the plain chain
+    (the refined EMI too: its routing and FP64 recomputation read the DS count on the device)."""
     cfg = CONFIGS["c1"].scaled(nlines=64, width=72, n_patches=6)
-    plain = DsChain(64, 72, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp, precision=prec,
-                    batch=900, device=cuda)
-    graph = DsChain(64, 72, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp, precision=prec,
-                    batch=900, device=cuda, graph=True)
+    kw = dict(precision=prec, emi_precision=emi_prec, batch=900, device=cuda)
+    plain = DsChain(64, 72, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp, **kw)
+    graph = DsChain(64, 72, cfg.nimages, cfg.az_half_win, cfg.r_half_win, cfg.p_max, cfg.min_shp, graph=True, **kw)
     for seed in (5, 6):
         z = make_stack(cfg.scaled(seed=seed), device=cuda)
         a, b = plain.run(z), graph.run(z)
@@ -641,6 +641,10 @@ def test_chain_in_cuda_graph(cuda, prec):
         assert torch.equal(b.t_coh.view(torch.int32), a.t_coh.view(torch.int32))
     with pytest.raises(ValueError):
         DsChain(8, 8, 200, 1, 1, graph=True, device=cuda)
+    with pytest.raises(ValueError):
+        DsChain(8, 8, 20, 1, 1, precision="fp64", emi_precision="mixed", graph=True, device=cuda)
+    with pytest.raises(ValueError):
+        DsChain(8, 8, 20, 1, 1, precision="fp64", emi_precision="refine", refine_tol=1e-3, graph=True, device=cuda)
 
 
 def test_ks_autotune_same_results(cuda):
