@@ -348,7 +348,7 @@ int size_class(int64_t npix) {
 
 std::vector<KsPlan> plan_candidates(int n, int azh, int rh) {
   std::vector<KsPlan> out;
-  for (size_t budget : {200u * 1024u, 100u * 1024u, 64u * 1024u, 40u * 1024u}) {
+  for (size_t budget : {200u * 1024u, 100u * 1024u, 64u * 1024u, 40u * 1024u, 28u * 1024u, 20u * 1024u}) {
     const KsPlan c = plan_ks(n, azh, rh, budget);
     if (c.th == 0) continue;
     bool dup = false;
